@@ -1,0 +1,97 @@
+"""Generate the golden fixtures in this directory from the UNMODIFIED reference.
+
+Run from the repository root after ``make -C oracle ref`` (which compiles the
+reference's own sources into ``oracle/_ref/``):
+
+    python tests/golden/make_golden.py
+
+For every case it writes ``<case>.fa`` (seeded synthetic input),
+``<case>.out`` (the reference CLI's stdout, byte for byte) and, where the case
+has per-call records, ``<case>.dump`` (one score + path per alignment() call,
+from ``oracle/ref_harness``). ``manifest.json`` lists the cases and options.
+The fixtures are kept small so the CPU test-suite stays fast; the full-size
+configurations are checked on the GPU through size-independent properties and
+against the CPU restatement.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from poa_b200 import synth  # noqa: E402
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "minipoa")
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+
+def edge_reads():
+    rng = np.random.default_rng(7)
+    t = synth.to_ascii(synth.random_root(rng, 300))
+    extra = synth.to_ascii(synth.random_root(rng, 120))
+    return {
+        # ragged lengths, an N run, lower case, a prefix, a 5 bp read, an
+        # extended read, a read with N, an unrelated (reversed) read
+        "edge_mixed": [t, t[:150] + b"NNNN" + t[154:], t.lower(), t[20:280], t[:5],
+                       t + extra, b"ACGTN", t[::-1][:200]],
+        "edge_single": [t],
+        "edge_empty_read": [t, b"", t[:100]],
+        "edge_all_n": [b"NNNNNNNN", b"NNNNN", t[:50]],
+        "edge_identical": [t[:200]] * 5,
+    }
+
+
+def cases():
+    out = []
+    out.append(("cons_small", synth.single_graph_consensus(seed=11, nseq=6, length=800), [], True))
+    out.append(("cons_scoring", synth.single_graph_consensus(seed=11, nseq=6, length=800),
+                ["-M", "3", "-X", "5", "-O", "6", "-E", "1", "-b", "20", "-f", "10"], True))
+    out.append(("cons_fullband", synth.single_graph_consensus(seed=16, nseq=5, length=400), ["-f", "0"], True))
+    out.append(("msa_small", synth.single_graph_msa(seed=12, nseq=8, length=700), ["-r", "1"], True))
+    noisy = synth.noisy_long_reads(seed=13, nreads=6, length=1200)
+    out.append(("noisy_adaptive", noisy, ["-B"], True))
+    out.append(("noisy_static", noisy, [], True))
+    out.append(("noisy_adaptive_msa", noisy, ["-B", "-r", "1"], False))
+    ws = synth.polishing_windows(seed=14, n_windows=10)
+    for w in range(ws.n_windows):
+        out.append((f"window_{w:02d}", ws.window_reads(w), [], w < 3))
+    lb = synth.windows(15, 3, (600, 600), (8, 12), 0.15, chimeric=0.1)
+    for w in range(lb.n_windows):
+        out.append((f"lbwindow_{w:02d}", lb.window_reads(w), ["-B"], w < 2))
+    for name, reads in edge_reads().items():
+        out.append((name, reads, [], True))
+        out.append((name + "_adaptive", reads, ["-B"], False))
+        out.append((name + "_msa", reads, ["-r", "1"], False))
+    seed_in = synth.single_graph_msa(seed=17, nseq=10, length=3000)
+    out.append(("seeded_msa", seed_in, ["-S", "-r", "1"], False))
+    out.append(("seeded_cons", seed_in, ["-S"], False))
+    return out
+
+
+def main():
+    if not (os.path.exists(REF_BIN) and os.path.exists(HARNESS)):
+        sys.exit("build the reference first: make -C oracle ref")
+    manifest = []
+    for name, reads, opts, dump in cases():
+        fa = os.path.join(HERE, name + ".fa")
+        synth.write_fasta(fa, reads)
+        res = subprocess.run([REF_BIN, fa] + opts, capture_output=True, check=True)
+        with open(os.path.join(HERE, name + ".out"), "wb") as fh:
+            fh.write(res.stdout)
+        if dump:
+            subprocess.run([HARNESS, fa] + opts + ["-d", os.path.join(HERE, name + ".dump")],
+                           capture_output=True, check=True)
+        manifest.append({"case": name, "opts": opts, "nseq": len(reads), "dump": dump})
+    with open(os.path.join(HERE, "manifest.json"), "w") as fh:
+        json.dump(manifest, fh, indent=1)
+    print(f"{len(manifest)} cases written")
+
+
+if __name__ == "__main__":
+    main()

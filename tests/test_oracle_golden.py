@@ -1,0 +1,33 @@
+"""The CPU restatement (oracle/) against the reference's own outputs.
+
+Every fixture in tests/golden/ was produced by the unmodified reference
+(oracle/_ref/minipoa and oracle/ref_harness, see tests/golden/make_golden.py).
+The restatement must reproduce the CLI output byte for byte and, where a
+per-call dump exists, every alignment() score and path.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+with open(os.path.join(GOLD, "manifest.json")) as fh:
+    MANIFEST = json.load(fh)
+# seeding (-S) is host-side minimizer chaining, checked by its own tests
+CASES = [c for c in MANIFEST if "-S" not in c["opts"]]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
+def test_restatement_matches_reference(case, oracle_bin, tmp_path):
+    fa = os.path.join(GOLD, case["case"] + ".fa")
+    args = [oracle_bin, fa] + case["opts"]
+    dump = tmp_path / "o.dump"
+    if case["dump"]:
+        args += ["-d", str(dump)]
+    res = subprocess.run(args, capture_output=True, check=True, timeout=120)
+    with open(os.path.join(GOLD, case["case"] + ".out"), "rb") as fh:
+        assert res.stdout == fh.read()
+    if case["dump"]:
+        with open(os.path.join(GOLD, case["case"] + ".dump"), "rb") as fh:
+            assert dump.read_bytes() == fh.read()

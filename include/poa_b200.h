@@ -1,0 +1,123 @@
+/*
+ * poa_b200.h - C ABI of the B200 partial-order-alignment engine.
+ *
+ * Plain pointers and sizes only. Every entry point returns a status code
+ * (POA_OK = 0) instead of exiting the process the way the reference does;
+ * poa_status_str() names it and poa_last_error() gives the last message of a
+ * context. Sequences are ASCII (A/C/G/T/N, either case) unless a parameter
+ * says "encoded" (codes 0..4 = A, C, G, T, N, as src/sequence.cpp:6-23).
+ *
+ * The entry points replace these reference interfaces (paths within the
+ * minipoa project):
+ *   poa_params / poa_params_init  para_t and its CLI defaults,
+ *                                 include/parameter.h:5-19, src/main.cpp:16-33,
+ *                                 normalised like initPara, src/handle_input.cpp:45-51
+ *   poa_align                     poa(), include/align.h:15, src/align.cpp:1353-1737
+ *   poa_run                       the driver loop + output, src/main.cpp:84-126
+ *                                 (alignment(), src/align.cpp:1741-1828; add_path,
+ *                                 topsort, output_consensus / output_rc_msa,
+ *                                 src/graph.cpp)
+ *   poa_batch_*                   the same driver over many independent windows
+ *                                 (no counterpart: the reference handles one
+ *                                 graph per process)
+ */
+#ifndef POA_B200_H
+#define POA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    POA_OK = 0,
+    POA_BAND_ESCAPE = 1, /* reference: prints the band and exit(0), src/align.cpp:1584-1588 */
+    POA_BT_FAIL = 2,     /* reference: " backtrack error" + exit(1), src/align.cpp:1730-1731 */
+    POA_BAD_ARG = 3,
+    POA_OOM = 4,         /* device memory exhausted */
+    POA_INDEGREE = 5,    /* a node with more than 510 in-window predecessors */
+    POA_DEGENERATE = 6,  /* an empty band / sub-window the reference cannot handle either */
+    POA_CAPACITY = 7,    /* a batched window outgrew its device graph capacity */
+    POA_CUDA = 8,        /* a CUDA runtime error; see poa_last_error() */
+    POA_UNSUPPORTED = 9
+};
+
+/* para_t, the fields on the path. Values are the raw CLI values; signs are
+ * normalised inside (initPara). */
+typedef struct {
+    int32_t match, mismatch, gap_open, gap_ext; /* -M -X -O -E: 2 -4 -4 -2 */
+    int32_t band_b, band_f;                     /* -b -f: 100 40 */
+    int32_t ab_band;                            /* -B: 0 */
+    int32_t seeding;                            /* -S: 0 */
+    int32_t k, mm_w, poa_w;                     /* -k -w -W: 19 10 10000 */
+    int32_t thread;                             /* -t: 1 */
+    int32_t result;                             /* -r: 0 consensus, 1 row-column MSA */
+    int32_t progressive;                        /* -p: 0 */
+    int32_t verbose;                            /* -V: 0 */
+} poa_params;
+
+typedef struct poa_ctx poa_ctx;
+
+void poa_params_init(poa_params* p);
+const char* poa_status_str(int status);
+
+/* One context per GPU and host thread; owns a CUDA stream and device memory. */
+poa_ctx* poa_create(int device, const poa_params* p);
+void poa_destroy(poa_ctx* ctx);
+const char* poa_last_error(const poa_ctx* ctx);
+void poa_free(void* ptr);
+
+/* The reference graph flattened (node_t, include/node.h:5-68; graph,
+ * include/graph.h:9-31). Arrays are indexed by node id unless stated. */
+typedef struct {
+    int32_t n_nodes;
+    const uint8_t* base;     /* encoded base */
+    const int32_t* rank;     /* node rank from the last topsort(op 0) */
+    const int32_t* par_id;
+    const int32_t* ind;      /* in-degree count incl. repeated edges */
+    const int32_t* aligned;  /* [n_nodes * 5] aligned_node */
+    const int32_t* in_ptr;   /* [n_nodes + 1] CSR in in-list order */
+    const int32_t* in_id;
+    const int32_t* in_weight;
+    const int32_t* out_ptr;  /* [n_nodes + 1] CSR in out-list order */
+    const int32_t* out_id;
+    int32_t n_ranks;
+    const int32_t* rank_to_id;
+    const int32_t* hlen;     /* by rank; may be NULL when band_f == 0 */
+    const int32_t* tlen;
+} poa_graph_view;
+
+/* res_t, include/result.h:3-12 */
+typedef struct {
+    int32_t from;
+    uint8_t base;
+    int32_t aligned_id;
+} poa_res;
+
+/* poa(): align the encoded query (qlen bases, codes 0..4) to ranks
+ * [rank(beg_id), rank(end_id)] of the graph; writes the forward path to out
+ * (capacity out_cap), its length to *out_len and the end-cell score to *score. */
+int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end_id, const uint8_t* q_enc,
+              int32_t qlen, int32_t ab_band, poa_res* out, int32_t out_cap, int32_t* out_len, int32_t* score);
+
+/* The whole minipoa run: reads in order, DP on the GPU, graph fusion on the
+ * host, output text exactly as minipoa prints it (consensus FASTA for
+ * result 0, one row per read for result 1). headers[i] is the text after '>'
+ * of read i ("name comment"), or NULL / "" for ">i+1". *text is allocated
+ * with malloc; release it with poa_free. scores (optional, nseq entries) gets
+ * the end-cell score of each read's last poa() call (0 for the first read). */
+int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
+            const char* const* headers, char** text, size_t* text_len, int32_t* scores);
+
+/* Counters since poa_create: [0] kernel launches, [1] alignments, [2] band
+ * cells, [3] kernel time in microseconds (when timing is on), [4] H2D bytes,
+ * [5] D2H bytes. */
+int poa_stats(const poa_ctx* ctx, int64_t* out6);
+int poa_set_timing(poa_ctx* ctx, int on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,175 @@
+"""poa_b200 - B200-native partial-order alignment (minipoa's hot path).
+
+The product is the native library ``libpoa_b200.so`` (CUDA kernels for
+sm_100a + the host driver in C++, behind the C ABI in include/poa_b200.h).
+This module is a thin ctypes mirror of that ABI for Python callers, tests
+and the benchmark. It never falls back to a CPU implementation: if the
+library is missing or no GPU is present, the calls raise.
+
+Mirrors the reference's operator interface (minipoa, src/main.cpp):
+``Params`` holds the CLI options with the same defaults, ``Context.run``
+is one minipoa invocation (consensus by default, row-column MSA with
+``result=1``), returning exactly the text minipoa prints.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpoa_b200.so")
+
+STATUS = {
+    0: "ok", 1: "backtrack left the band", 2: "backtrack error", 3: "bad argument",
+    4: "out of device memory", 5: "node in-degree above 510 within one window",
+    6: "degenerate band or sub-window", 7: "window outgrew its device capacity",
+    8: "CUDA error", 9: "unsupported option",
+}
+
+
+class PoaError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        super().__init__(f"poa status {status} ({STATUS.get(status, '?')}){': ' + msg if msg else ''}")
+        self.status = status
+
+
+class _CParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "match", "mismatch", "gap_open", "gap_ext", "band_b", "band_f", "ab_band", "seeding",
+        "k", "mm_w", "poa_w", "thread", "result", "progressive", "verbose")]
+
+
+@dataclass
+class Params:
+    """minipoa's options (src/main.cpp:16-33) with the same defaults."""
+    match: int = 2          # -M
+    mismatch: int = -4      # -X
+    gap_open: int = -4      # -O
+    gap_ext: int = -2       # -E
+    band_b: int = 100       # -b
+    band_f: int = 40        # -f
+    ab_band: bool = False   # -B
+    seeding: bool = False   # -S
+    k: int = 19             # -k
+    mm_w: int = 10          # -w
+    poa_w: int = 10000      # -W
+    thread: int = 1         # -t
+    result: int = 0         # -r (0 consensus, 1 MSA)
+    progressive: bool = False  # -p
+    verbose: int = 0        # -V
+
+    def _c(self) -> _CParams:
+        return _CParams(*[int(getattr(self, f[0])) for f in _CParams._fields_])
+
+    @classmethod
+    def from_cli(cls, opts: Sequence[str]) -> "Params":
+        """Parse minipoa-style short options (``-B -r 1 -M 3 ...``)."""
+        keys = {"-M": "match", "-X": "mismatch", "-O": "gap_open", "-E": "gap_ext", "-b": "band_b",
+                "-f": "band_f", "-k": "k", "-w": "mm_w", "-W": "poa_w", "-t": "thread", "-r": "result",
+                "-V": "verbose"}
+        flags = {"-B": "ab_band", "-S": "seeding", "-p": "progressive"}
+        p = cls()
+        it = iter(opts)
+        for o in it:
+            if o in flags:
+                setattr(p, flags[o], True)
+            elif o in keys:
+                setattr(p, keys[o], int(next(it)))
+            else:
+                raise ValueError(f"unknown option {o}")
+        return p
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m poa_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.poa_params_init.argtypes = [ctypes.POINTER(_CParams)]
+    L.poa_create.restype = ctypes.c_void_p
+    L.poa_create.argtypes = [ctypes.c_int, ctypes.POINTER(_CParams)]
+    L.poa_destroy.argtypes = [ctypes.c_void_p]
+    L.poa_last_error.restype = ctypes.c_char_p
+    L.poa_last_error.argtypes = [ctypes.c_void_p]
+    L.poa_status_str.restype = ctypes.c_char_p
+    L.poa_free.argtypes = [ctypes.c_void_p]
+    L.poa_run.restype = ctypes.c_int
+    L.poa_run.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_char_p),
+                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_char_p),
+                          ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
+                          ctypes.POINTER(ctypes.c_int32)]
+    L.poa_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+    L.poa_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    _lib = L
+    return L
+
+
+class Context:
+    """One device context (CUDA stream + device arena) with fixed options."""
+
+    def __init__(self, params: Optional[Params] = None, device: int = 0):
+        self.params = params or Params()
+        L = lib()
+        self._cp = self.params._c()
+        self._h = L.poa_create(device, ctypes.byref(self._cp))
+        if not self._h:
+            raise PoaError(8, "poa_create failed (no CUDA device or out of memory)")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().poa_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            raise PoaError(st, lib().poa_last_error(self._h).decode(errors="replace"))
+
+    def run(self, seqs: Sequence[bytes], headers: Optional[Sequence[str]] = None) -> Tuple[bytes, List[int]]:
+        """One minipoa run over ``seqs``; returns (stdout text, per-read score)."""
+        n = len(seqs)
+        arr = (ctypes.c_char_p * n)(*[bytes(s) for s in seqs])
+        lens = (ctypes.c_int32 * n)(*[len(s) for s in seqs])
+        hdr = None
+        if headers is not None:
+            hdr = (ctypes.c_char_p * n)(*[h.encode() for h in headers])
+        out = ctypes.c_void_p()
+        olen = ctypes.c_size_t()
+        scores = (ctypes.c_int32 * max(n, 1))()
+        st = lib().poa_run(self._h, n, arr, lens, hdr, ctypes.byref(out), ctypes.byref(olen), scores)
+        self._check(st)
+        text = ctypes.string_at(out.value, olen.value)
+        lib().poa_free(out)
+        return text, list(scores)[:n]
+
+    def set_timing(self, on: bool = True):
+        lib().poa_set_timing(self._h, 1 if on else 0)
+
+    def stats(self) -> dict:
+        o = (ctypes.c_int64 * 6)()
+        lib().poa_stats(self._h, o)
+        return dict(launches=o[0], alignments=o[1], cells=o[2], kernel_us=o[3], h2d_bytes=o[4], d2h_bytes=o[5])
+
+
+def run(seqs: Sequence[bytes], params: Optional[Params] = None, headers=None, device: int = 0) -> bytes:
+    with Context(params, device) as ctx:
+        return ctx.run(seqs, headers)[0]

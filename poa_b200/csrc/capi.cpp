@@ -1,0 +1,244 @@
+// capi.cpp - the extern "C" boundary (include/poa_b200.h). No exception or
+// C++ type crosses it: failures become status codes plus a per-context
+// message.
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/poa_b200.h"
+#include "gpu_engine.h"
+
+struct poa_ctx {
+    int device = 0;
+    pb::Params p;
+    pb::GpuEngine* eng = nullptr;
+    std::string err;
+};
+
+namespace {
+
+pb::Params to_params(const poa_params* c) {
+    pb::Params p;
+    p.match = c->match;
+    p.mismatch = c->mismatch;
+    p.gap_open1 = c->gap_open;
+    p.gap_ext1 = c->gap_ext;
+    p.b = c->band_b;
+    p.f = c->band_f;
+    p.ab_band = c->ab_band;
+    p.enable_seeding = c->seeding;
+    p.k = c->k;
+    p.mm_w = c->mm_w;
+    p.poa_w = c->poa_w;
+    p.thread = c->thread;
+    p.result = c->result;
+    p.progressive = c->progressive;
+    p.verbose = c->verbose;
+    pb::normalize_params(p);
+    return p;
+}
+
+int fail(poa_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+// Window view of ranks [rank(beg), rank(end)] straight from the flat graph.
+void window_from_view(const poa_graph_view& g, int beg_id, int end_id, bool with_lens, pb::HostWindow& w) {
+    const int beg_i = g.rank[beg_id], end_i = g.rank[end_id];
+    const int n = end_i - beg_i + 1;
+    w.n = n;
+    w.beg_i = beg_i;
+    w.end_i = end_i;
+    w.max_indeg = 0;
+    if (n <= 0) return;
+    w.row_node.resize(n);
+    w.base.resize(n);
+    w.ind.resize(n);
+    w.hq.assign(n, 0);
+    w.hq_loc.assign(n, 0);
+    w.tq.assign(n, 0);
+    w.in_ptr.assign(n + 1, 0);
+    w.out_ptr.assign(n + 1, 0);
+    w.in_row.clear(); w.in_w.clear(); w.in_base.clear(); w.out_row.clear();
+    for (int r = 0; r < n; r++) {
+        const int u = g.rank_to_id[beg_i + r];
+        w.row_node[r] = u;
+        w.base[r] = g.base[u];
+        w.ind[r] = g.ind[u];
+        if (with_lens) {
+            w.hq[r] = g.hlen[beg_i + r] - g.hlen[beg_i];
+            w.hq_loc[r] = g.hlen[r] - g.hlen[beg_i];
+            w.tq[r] = g.tlen[beg_i + r] - g.tlen[end_i];
+        }
+        int deg = 0;
+        for (int e = g.in_ptr[u]; e < g.in_ptr[u + 1]; e++) {
+            int p = g.rank[g.in_id[e]] - beg_i;
+            if (p < 0) continue;
+            w.in_row.push_back(p);
+            w.in_w.push_back(g.in_weight[e]);
+            w.in_base.push_back(p == 0 ? 4 : g.base[g.in_id[e]]);
+            deg++;
+        }
+        if (deg > w.max_indeg) w.max_indeg = deg;
+        w.in_ptr[r + 1] = (int32_t)w.in_row.size();
+        for (int e = g.out_ptr[u]; e < g.out_ptr[u + 1]; e++) {
+            int s = g.rank[g.out_id[e]] - beg_i;
+            if (s >= n) continue;
+            w.out_row.push_back(s);
+        }
+        w.out_ptr[r + 1] = (int32_t)w.out_row.size();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void poa_params_init(poa_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->match = 2; p->mismatch = -4; p->gap_open = -4; p->gap_ext = -2;
+    p->band_b = 100; p->band_f = 40;
+    p->k = 19; p->mm_w = 10; p->poa_w = 10000;
+    p->thread = 1;
+}
+
+const char* poa_status_str(int s) {
+    switch (s) {
+        case POA_OK: return "ok";
+        case POA_BAND_ESCAPE: return "backtrack left the band";
+        case POA_BT_FAIL: return "backtrack error";
+        case POA_BAD_ARG: return "bad argument";
+        case POA_OOM: return "out of device memory";
+        case POA_INDEGREE: return "node in-degree above 510 within one window";
+        case POA_DEGENERATE: return "degenerate band or sub-window";
+        case POA_CAPACITY: return "window outgrew its device capacity";
+        case POA_CUDA: return "CUDA error";
+        case POA_UNSUPPORTED: return "unsupported option";
+        default: return "unknown status";
+    }
+}
+
+poa_ctx* poa_create(int device, const poa_params* p) {
+    poa_ctx* ctx = new (std::nothrow) poa_ctx;
+    if (!ctx) return nullptr;
+    try {
+        poa_params d;
+        poa_params_init(&d);
+        ctx->p = to_params(p ? p : &d);
+        ctx->device = device;
+        ctx->eng = new pb::GpuEngine(device);
+    } catch (const std::exception& e) {
+        delete ctx->eng;
+        delete ctx;
+        return nullptr;
+    }
+    return ctx;
+}
+
+void poa_destroy(poa_ctx* ctx) {
+    if (!ctx) return;
+    delete ctx->eng;
+    delete ctx;
+}
+
+const char* poa_last_error(const poa_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void poa_free(void* ptr) { std::free(ptr); }
+
+int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end_id, const uint8_t* q_enc,
+              int32_t qlen, int32_t ab_band, poa_res* out, int32_t out_cap, int32_t* out_len, int32_t* score) {
+    if (!ctx || !g || (!q_enc && qlen > 0) || qlen < 0 || !out || !out_len || !score)
+        return fail(ctx, POA_BAD_ARG, "null argument");
+    if (beg_id < 0 || end_id < 0 || beg_id >= g->n_nodes || end_id >= g->n_nodes)
+        return fail(ctx, POA_BAD_ARG, "node id out of range");
+    try {
+        pb::HostWindow w;
+        const bool lens = ctx->p.f > 0;
+        if (lens && (!g->hlen || !g->tlen)) return fail(ctx, POA_BAD_ARG, "hlen/tlen required when band_f > 0");
+        window_from_view(*g, beg_id, end_id, lens, w);
+        if (w.n <= 0) return fail(ctx, POA_DEGENERATE, "end rank precedes begin rank");
+        std::vector<pb::AlignOut> outs;
+        ctx->eng->align_many({&w}, {q_enc}, {qlen}, {ab_band}, ctx->p, outs);
+        if (outs[0].status != POA_OK) return fail(ctx, outs[0].status, poa_status_str(outs[0].status));
+        const std::vector<int32_t>& mv = outs[0].moves;
+        if ((int32_t)mv.size() > out_cap) return fail(ctx, POA_BAD_ARG, "output capacity too small");
+        int k = 0;
+        for (int t = (int)mv.size() - 1; t >= 0; t--, k++) {
+            const int kind = pb::mv_kind(mv[t]), qc = pb::mv_qc(mv[t]);
+            poa_res r;
+            r.base = (uint8_t)qc;
+            r.from = -1;
+            r.aligned_id = -1;
+            if (kind != pb::MV_INSERT) {
+                const int pre = w.row_node[pb::mv_row(mv[t])];
+                if (kind == pb::MV_MATCH) {
+                    r.from = pre;
+                    r.base = g->base[pre];
+                } else {
+                    const int par = g->par_id[pre];
+                    const int al = g->aligned[par * 5 + qc];
+                    if (al != -1) r.from = al;
+                    else r.aligned_id = par;
+                }
+            }
+            out[k] = r;
+        }
+        *out_len = k;
+        *score = outs[0].score;
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+}
+
+int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
+            const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
+    if (!ctx || nseq < 0 || (nseq > 0 && (!seqs || !lens)) || !text) return fail(ctx, POA_BAD_ARG, "null argument");
+    try {
+        std::vector<std::string> s(nseq), h;
+        for (int i = 0; i < nseq; i++) {
+            if (lens[i] < 0 || (lens[i] > 0 && !seqs[i])) return fail(ctx, POA_BAD_ARG, "bad sequence");
+            s[i].assign(seqs[i] ? seqs[i] : "", (size_t)lens[i]);
+        }
+        if (headers) {
+            h.resize(nseq);
+            for (int i = 0; i < nseq; i++) h[i] = headers[i] ? headers[i] : "";
+        }
+        std::string out;
+        std::vector<int32_t> sc;
+        int st = pb::run_reads(ctx->p, s, h, *ctx->eng, out, scores ? &sc : nullptr, nullptr);
+        if (st != POA_OK) return fail(ctx, st, poa_status_str(st));
+        char* buf = (char*)std::malloc(out.size() + 1);
+        if (!buf) return fail(ctx, POA_BAD_ARG, "host allocation failed");
+        std::memcpy(buf, out.data(), out.size());
+        buf[out.size()] = 0;
+        *text = buf;
+        if (text_len) *text_len = out.size();
+        if (scores) {
+            // one entry per read: reads whose alignment ran on an empty graph get 0
+            int first_dp = nseq - (int)sc.size();
+            for (int i = 0; i < nseq; i++) scores[i] = i >= first_dp ? sc[i - first_dp] : 0;
+        }
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+}
+
+int poa_stats(const poa_ctx* ctx, int64_t* o) {
+    if (!ctx || !o) return POA_BAD_ARG;
+    const pb::EngineStats& s = ctx->eng->stats;
+    o[0] = s.launches; o[1] = s.alignments; o[2] = s.cells;
+    o[3] = (int64_t)(s.kernel_ms * 1000.0); o[4] = s.h2d_bytes; o[5] = s.d2h_bytes;
+    return POA_OK;
+}
+
+int poa_set_timing(poa_ctx* ctx, int on) {
+    if (!ctx) return POA_BAD_ARG;
+    ctx->eng->timing = on != 0;
+    return POA_OK;
+}
+
+}  // extern "C"

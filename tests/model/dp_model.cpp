@@ -1,0 +1,215 @@
+// dp_model.cpp - TEST-ONLY sequential model of the CUDA DP kernels.
+//
+// It runs exactly the per-block steps of plain.cu (pass 1 over predecessors,
+// prefix-max scan, finalisation, backtrack records, row store layout, the
+// record-driven backtrack) one block at a time on the CPU, using the same
+// dp_core.h / dp_rowops.h functions the kernels use. The tests compare it with
+// the oracle on every golden case; that validates the kernel formulation
+// (scan form of the I recurrence, block masks, compact records) before any
+// GPU run. It is never linked into the product library.
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "driver.h"
+#include "dp_rowops.h"
+
+using namespace pb;
+
+namespace {
+
+int64_t align16(int64_t x) { return (x + 15) / 16 * 16; }
+
+struct ModelEngine : DpEngine {
+    std::vector<int32_t> rs;
+    std::vector<uint8_t> tb;
+
+    void align_many(const std::vector<const HostWindow*>& wins, const std::vector<const uint8_t*>& qs,
+                    const std::vector<int32_t>& qlens, const std::vector<int32_t>& abs, const Params& p,
+                    std::vector<AlignOut>& outs) override {
+        outs.assign(wins.size(), AlignOut());
+        for (size_t t = 0; t < wins.size(); t++) run(*wins[t], qs[t], qlens[t], abs[t], p, outs[t]);
+    }
+
+    void run(const HostWindow& hw, const uint8_t* q, int qlen, int ab, const Params& p, AlignOut& o) {
+        const int n = hw.n, m = qlen + 1;
+        std::vector<uint8_t> qsb(qs_bytes(qlen));
+        make_qs(q, qlen, qsb.data());
+        std::vector<RowMeta> meta(n);
+        std::vector<int32_t> state((size_t)AB_NSTATE * n);
+        std::vector<int32_t> moves(n + m + 8);
+        int32_t out[4] = {0, 0, 0, 0};
+        DpArgs a;
+        a.v = WinView{n, hw.in_ptr.data(), hw.in_row.data(), hw.in_w.data(), hw.in_base.data(), hw.base.data(),
+                      hw.ind.data(), hw.hq.data(), hw.hq_loc.data(), hw.tq.data(), hw.out_ptr.data(),
+                      hw.out_row.data()};
+        a.qs = qsb.data();
+        a.qlen = qlen;
+        a.ab_band = ab;
+        a.f = p.f;
+        a.w = p.b + (p.f ? m / p.f : 0);
+        a.sc = scoring_of(p);
+        a.meta = meta.data();
+        a.state = state.data();
+        a.moves = moves.data();
+        a.moves_cap = (int32_t)moves.size();
+        a.out = out;
+        // generous capacity: every row at full width
+        int64_t full_blocks = (int64_t)(m / BLK + 2);
+        rs.assign((size_t)(n * full_blocks * 16 + 16), 0);
+        tb.assign((size_t)(n * (full_blocks * BLK * 4 + 16) + 16), 0);
+        a.rs = rs.data();
+        a.rs_cap = (int64_t)rs.size();
+        a.tb = tb.data();
+        a.tb_cap = (int64_t)tb.size();
+        fill(a, m);
+        o.status = out[0];
+        o.score = out[1];
+        o.cells = out[3];
+        if (o.status == ST_OK) {
+            int32_t nm = 0;
+            o.status = backtrack_records(a, m, nm);
+            o.moves.assign(moves.begin(), moves.begin() + nm);
+        }
+    }
+
+    static void fill(DpArgs& a, int m) {
+        const int n = a.v.n;
+        const Scoring sc = a.sc;
+        const bool adaptive = a.f > 0 && a.ab_band;
+        if (adaptive)
+            for (int r = 0; r < n; r++) adaptive_init_entry(a, r, m);
+        int64_t st_next = 0, tb_next = 0, cells = 0;
+        std::vector<int32_t> H0, Dk, Mf, If;
+        for (int i = 0; i < n; i++) {
+            int Bs, Be;
+            row_band(a, i, m, Bs, Be);
+            if (i == 0) Bs = 0;  // row 0 always starts at column 0 (Ms[0] = 0)
+            const int bn = Be - Bs - 1;
+            if (bn < 0) { a.out[0] = ST_DEGENERATE; return; }
+            const int e0 = a.v.in_ptr[i], d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
+            if (d > MAX_MULTI_PRED) { a.out[0] = ST_INDEGREE; return; }
+            const int bpc = d >= 2 ? 4 : 1;
+            RowMeta rm{Bs, Be, st_next, tb_next};
+            if (st_next + (int64_t)bn * 16 > a.rs_cap || tb_next + (int64_t)bn * BLK * bpc > a.tb_cap) {
+                a.out[0] = ST_OOM;
+                return;
+            }
+            a.meta[i] = rm;
+            cells += (int64_t)bn * BLK;
+            H0.assign((size_t)bn * BLK, 0);
+            Dk.assign((size_t)bn * BLK, 0);
+            Mf.assign((size_t)bn * BLK, 0);
+            If.assign((size_t)bn * BLK, 0);
+            // pass 1
+            for (int b = 0; b < bn; b++) {
+                const int B = Bs + b;
+                int32_t Mpre[BLK], Dv[BLK];
+                for (int l = 0; l < BLK; l++) Mpre[l] = Dv[l] = NEG_INF;
+                if (i == 0) {
+                    for (int l = 0; l < BLK; l++) Mpre[l] = (b * BLK + l == 0) ? 0 : NEG_INF;
+                }
+                const uint8_t* qc8 = a.qs + (int64_t)B * BLK;
+                for (int e = e0; e < e0 + d; e++) {
+                    const int pr = a.v.in_row[e];
+                    const RowMeta pm = a.meta[pr];
+                    PredMask mk = pred_mask(B, pm.Bs, pm.Be);
+                    const int32_t* Mb = a.rs + pm.st + (int64_t)(B - pm.Bs) * 16;
+                    int32_t mprev = mk.prev_in ? a.rs[pm.st + (int64_t)(B - 1 - pm.Bs) * 16 + 7] : NEG_INF;
+                    if (mk.blk_in) pass1_pred(sc, mk, b == 0, a.v.in_base[e], Mb, Mb + 8, mprev, qc8, Mpre, Dv);
+                }
+                for (int l = 0; l < BLK; l++) {
+                    H0[b * BLK + l] = mx(Mpre[l], Dv[l]);
+                    Dk[b * BLK + l] = Dv[l];
+                }
+            }
+            // scan + finalise (row 0: M = H0 exactly, I = NEG_INF)
+            int32_t P = 0;
+            for (int b = 0; b < bn; b++) {
+                int32_t* M = &Mf[b * BLK];
+                int32_t* I = &If[b * BLK];
+                if (i == 0) {
+                    for (int l = 0; l < BLK; l++) { M[l] = H0[b * BLK + l]; I[l] = NEG_INF; }
+                } else {
+                    finalize_block(sc, b * BLK, P, &H0[b * BLK], M, I);
+                }
+                for (int l = 0; l < BLK; l++) {
+                    int32_t key = scan_key(H0[b * BLK + l], b * BLK + l, sc.e1);
+                    P = (b == 0 && l == 0) ? key : mx(P, key);
+                }
+            }
+            // records + store
+            for (int b = 0; b < bn; b++) {
+                const int B = Bs + b;
+                const int32_t* M = &Mf[b * BLK];
+                const int32_t* I = &If[b * BLK];
+                const int32_t* D = &Dk[b * BLK];
+                const uint8_t* qc8 = a.qs + (int64_t)B * BLK;
+                FlagAcc acc;
+                flag_acc_init(acc);
+                for (int e = e0; e < e0 + d; e++) {
+                    const int pr = a.v.in_row[e];
+                    const RowMeta pm = a.meta[pr];
+                    PredMask mk = pred_mask(B, pm.Bs, pm.Be);
+                    const int32_t* Mb = a.rs + pm.st + (int64_t)(B - pm.Bs) * 16;
+                    int32_t mprev = mk.prev_in ? a.rs[pm.st + (int64_t)(B - 1 - pm.Bs) * 16 + 7] : NEG_INF;
+                    if (mk.blk_in || mk.prev_in)
+                        flags_pred(sc, mk, a.v.in_base[e], a.v.in_w[e], e - e0, Mb, Mb + 8, mprev, qc8, M, D, acc);
+                }
+                int32_t* dst = a.rs + rm.st + (int64_t)b * 16;
+                for (int l = 0; l < BLK; l++) {
+                    const int j = b * BLK + l;
+                    int32_t Ml = j > 0 ? Mf[j - 1] : NEG_INF, Il = j > 0 ? If[j - 1] : NEG_INF;
+                    uint32_t own = own_flags(sc, j, M[l], D[l], I[l], Ml, Il);
+                    if (bpc == 1) a.tb[rm.tb + j] = encode_small(own, acc, l, a.v.ind[i]);
+                    else *(uint32_t*)(a.tb + rm.tb + (int64_t)j * 4) = encode_wide(own, acc, l, a.v.ind[i]);
+                    dst[l] = M[l];
+                    dst[8 + l] = D[l];
+                }
+            }
+            if (adaptive && i >= 1) {
+                int max_j = 0;
+                for (int j = 1; j < bn * BLK; j++) max_j = Mf[j] > Mf[max_j] ? j : max_j;
+                adaptive_update(a, i, Bs, max_j);
+            }
+            st_next += (int64_t)bn * 16;
+            tb_next = align16(tb_next + (int64_t)bn * BLK * bpc);
+        }
+        const RowMeta last = a.meta[n - 1];
+        const int jm = m - last.Bs * BLK;
+        a.out[1] = a.rs[last.st + (int64_t)(jm / BLK) * 16 + jm % BLK];
+        a.out[3] = (int32_t)std::min<int64_t>(cells, INT32_MAX);
+        a.out[0] = ST_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+// Run the whole driver with the model engine. params: match, mismatch,
+// gap_open, gap_ext, b, f, ab_band, result. Returns status; *text is malloc'd.
+int model_run(int nseq, const char* const* seqs, const int* lens, const int* params, char** text,
+              int* scores) {
+    Params p;
+    p.match = params[0]; p.mismatch = params[1]; p.gap_open1 = params[2]; p.gap_ext1 = params[3];
+    p.b = params[4]; p.f = params[5]; p.ab_band = params[6]; p.result = params[7];
+    normalize_params(p);
+    std::vector<std::string> s(nseq), headers;
+    for (int i = 0; i < nseq; i++) s[i].assign(seqs[i], lens[i]);
+    ModelEngine eng;
+    std::string out;
+    std::vector<int32_t> sc;
+    int st = run_reads(p, s, headers, eng, out, &sc, nullptr);
+    *text = (char*)malloc(out.size() + 1);
+    memcpy(*text, out.data(), out.size());
+    (*text)[out.size()] = 0;
+    if (scores)
+        for (size_t i = 0; i < sc.size(); i++) scores[i] = sc[i];
+    return st;
+}
+
+void model_free(void* p) { free(p); }
+}

@@ -111,6 +111,28 @@ int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end
 int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
             const char* const* headers, char** text, size_t* text_len, int32_t* scores);
 
+/* Batched windows (consensus mode, no -S/-p): many independent read sets,
+ * one POA graph and one consensus each, all in one persistent launch on the
+ * device; no counterpart in the reference, which handles one graph per
+ * process (each window equals one minipoa run on its reads).
+ * Reads are ASCII, read r = seq[read_off[r] .. read_off[r] + read_len[r]);
+ * window w owns reads win_off[w] .. win_off[w+1]-1, aligned in that order.
+ * poa_batch_upload copies them into device memory (kept resident),
+ * poa_batch_run runs every window and returns the device time in ms, and
+ * poa_batch_download writes window w's consensus to
+ * cons[cons_off[w] .. cons_off[w+1]) (cons_cap bytes available; cons_off has
+ * n_windows + 1 entries) and its status. poa_batch_consensus does all three. */
+int poa_batch_upload(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                     const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows);
+int poa_batch_run(poa_ctx* ctx, double* device_ms);
+int poa_batch_download(poa_ctx* ctx, char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status);
+int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                        const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows,
+                        char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status);
+/* [0] band cells of the last run, [1] windows that failed, [2] concurrent
+ * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes. */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out6);
+
 /* Counters since poa_create: [0] kernel launches, [1] alignments, [2] band
  * cells, [3] kernel time in microseconds (when timing is on), [4] H2D bytes,
  * [5] D2H bytes. */

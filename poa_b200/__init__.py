@@ -107,6 +107,14 @@ def lib() -> ctypes.CDLL:
                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
                           ctypes.POINTER(ctypes.c_int32)]
     L.poa_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+    _i64p, _i32p, _u8p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p
+    L.poa_batch_upload.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _i64p, _i32p, ctypes.c_int32, _i32p,
+                                   ctypes.c_int32]
+    L.poa_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    L.poa_batch_download.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i64p, _i32p]
+    L.poa_batch_consensus.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _i64p, _i32p, ctypes.c_int32, _i32p,
+                                      ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, _i64p, _i32p]
+    L.poa_batch_stats.argtypes = [ctypes.c_void_p, _i64p]
     L.poa_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     _lib = L
     return L
@@ -160,6 +168,67 @@ class Context:
         text = ctypes.string_at(out.value, olen.value)
         lib().poa_free(out)
         return text, list(scores)[:n]
+
+    # ---- batched windows -------------------------------------------------
+    @staticmethod
+    def _win_arrays(ws):
+        import numpy as np
+        seq = np.ascontiguousarray(ws.seq, dtype=np.uint8)
+        roff = np.ascontiguousarray(ws.read_off, dtype=np.int64)
+        rlen = np.ascontiguousarray(ws.read_len, dtype=np.int32)
+        woff = np.ascontiguousarray(ws.win_off, dtype=np.int32)
+        return seq, roff, rlen, woff
+
+    def batch_upload(self, ws) -> None:
+        """Copy a synth.WindowSet-like batch (seq, read_off, read_len, win_off) to the device."""
+        seq, roff, rlen, woff = self._keep = self._win_arrays(ws)
+        i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        st = lib().poa_batch_upload(self._h, seq.ctypes.data, seq.shape[0], roff.ctypes.data_as(i64p),
+                                    rlen.ctypes.data_as(i32p), rlen.shape[0], woff.ctypes.data_as(i32p),
+                                    woff.shape[0] - 1)
+        self._check(st)
+        self._nwin = int(woff.shape[0] - 1)
+        self._cons_cap = int(2 * (int(rlen.max()) if rlen.shape[0] else 0) + 64) * max(self._nwin, 1)
+
+    def batch_run(self) -> float:
+        """Run every uploaded window on the device; returns the device time (ms)."""
+        ms = ctypes.c_double()
+        self._check(lib().poa_batch_run(self._h, ctypes.byref(ms)))
+        return ms.value
+
+    def batch_download(self):
+        """(consensus bytes per window, status per window) of the last run."""
+        import numpy as np
+        cons = ctypes.create_string_buffer(max(self._cons_cap, 1))
+        off = np.zeros(self._nwin + 1, dtype=np.int64)
+        st = np.zeros(max(self._nwin, 1), dtype=np.int32)
+        self._check(lib().poa_batch_download(self._h, cons, self._cons_cap,
+                                             off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                             st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        raw = cons.raw
+        return [raw[off[w]:off[w + 1]] for w in range(self._nwin)], [int(x) for x in st[:self._nwin]]
+
+    def batch_consensus(self, ws):
+        """Upload + run + download through poa_batch_consensus (host buffers in, host buffers out)."""
+        import numpy as np
+        seq, roff, rlen, woff = self._win_arrays(ws)
+        nwin = int(woff.shape[0] - 1)
+        cap = int(2 * (int(rlen.max()) if rlen.shape[0] else 0) + 64) * max(nwin, 1)
+        cons = ctypes.create_string_buffer(max(cap, 1))
+        off = np.zeros(nwin + 1, dtype=np.int64)
+        st = np.zeros(max(nwin, 1), dtype=np.int32)
+        i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        self._check(lib().poa_batch_consensus(self._h, seq.ctypes.data, seq.shape[0], roff.ctypes.data_as(i64p),
+                                              rlen.ctypes.data_as(i32p), rlen.shape[0], woff.ctypes.data_as(i32p),
+                                              nwin, cons, cap, off.ctypes.data_as(i64p), st.ctypes.data_as(i32p)))
+        self._nwin = nwin
+        raw = cons.raw
+        return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
+
+    def batch_stats(self) -> dict:
+        o = (ctypes.c_int64 * 6)()
+        self._check(lib().poa_batch_stats(self._h, o))
+        return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5])
 
     def set_timing(self, on: bool = True):
         lib().poa_set_timing(self._h, 1 if on else 0)

@@ -1,0 +1,636 @@
+// batch.cu - persistent batched POA over independent windows (see batch.h).
+//
+// Device graph. A window's graph lives in its warp's slot as flat arrays with
+// fixed capacities: per node base, par_id, aligned_node[5], in-degree count,
+// rank and the heads/tails of two singly linked edge lists (in-list and
+// out-list, kept in insertion order exactly like node_t's vectors); per edge
+// its endpoints, weight and the next links of both lists. Fusion
+// (src/graph.cpp:170-235), the LIFO topological sort with hlen/tlen
+// (src/graph.cpp:21-128) and the consensus (src/graph.cpp:294-351) are the
+// reference's sequential algorithms, run by lane 0; the window view of the
+// DP rows, the shifted query and the DP fill itself use the whole warp.
+#include "batch.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+#include "gpu_engine.h"
+#include "plain.cuh"
+
+namespace pb {
+
+namespace {
+
+inline size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct SlotLayout {
+    int32_t NC, EC, QC;         // node, edge and query capacities
+    int32_t ring_rows, ring_blocks;
+    int64_t rs_cap, tb_cap;     // int32 units / bytes
+    // byte offsets inside a slot
+    int64_t hdr, base, par, aligned, ind, rank, in_head, in_tail, out_head, out_tail, in_cnt, out_cnt;
+    int64_t e_from, e_to, e_w, e_nin, e_nout;
+    int64_t rank_to_id, hlen, tlen, deg, stk, pre, score;
+    int64_t v_in_ptr, v_in_row, v_in_w, v_in_base, v_out_ptr, v_out_row, v_base, v_ind, v_hq, v_hq_loc, v_tq;
+    int64_t meta, state, qs, moves, rs, tb;
+    int64_t bytes;
+};
+
+SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, int32_t ring_blocks, int64_t spill_rows,
+                       int64_t tb_cap, bool adaptive) {
+    SlotLayout L;
+    L.NC = NC; L.EC = EC; L.QC = QC;
+    L.ring_rows = ring_rows; L.ring_blocks = ring_blocks;
+    L.rs_cap = (int64_t)ring_rows * ring_blocks * 16 + spill_rows * ring_blocks * 16;
+    L.tb_cap = tb_cap;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t r = o; o = up256(o + bytes); return (int64_t)r; };
+    const size_t n4 = 4 * (size_t)NC, e4 = 4 * (size_t)EC;
+    L.hdr = take(64);
+    L.base = take(NC); L.par = take(n4); L.aligned = take(5 * n4); L.ind = take(n4); L.rank = take(n4);
+    L.in_head = take(n4); L.in_tail = take(n4); L.out_head = take(n4); L.out_tail = take(n4);
+    L.in_cnt = take(n4); L.out_cnt = take(n4);
+    L.e_from = take(e4); L.e_to = take(e4); L.e_w = take(e4); L.e_nin = take(e4); L.e_nout = take(e4);
+    L.rank_to_id = take(n4); L.hlen = take(n4); L.tlen = take(n4); L.deg = take(n4); L.stk = take(n4);
+    L.pre = take(n4); L.score = take(n4);
+    L.v_in_ptr = take(n4 + 4); L.v_in_row = take(e4); L.v_in_w = take(e4); L.v_in_base = take(EC);
+    L.v_out_ptr = take(n4 + 4); L.v_out_row = take(e4); L.v_base = take(NC); L.v_ind = take(n4);
+    L.v_hq = take(n4); L.v_hq_loc = take(n4); L.v_tq = take(n4);
+    L.meta = take(sizeof(RowMeta) * (size_t)NC);
+    L.state = take(adaptive ? 4 * (size_t)AB_NSTATE * NC : 64);
+    L.qs = take((size_t)qs_bytes(QC) + 64);
+    L.moves = take(4 * ((size_t)NC + QC + 16));
+    L.rs = take(4 * (size_t)L.rs_cap);
+    L.tb = take((size_t)tb_cap);
+    L.bytes = (int64_t)up256(o);
+    return L;
+}
+
+struct BatchArgs {
+    const uint8_t* seq;
+    const int64_t* read_off;
+    const int32_t* read_len;
+    const int32_t* win_off;
+    const int32_t* order;
+    int32_t* counter;
+    int32_t n_windows;
+    Scoring sc;
+    int32_t b, f, ab_band;
+    char* slots;
+    SlotLayout L;
+    char* cons;
+    int32_t cons_stride;
+    int32_t* cons_len;
+    int32_t* status;
+    int64_t* cells;
+};
+
+// Pointers of one slot's device graph.
+struct DevGraph {
+    int32_t* hdr;  // [0] nodes, [1] edges
+    uint8_t* base;
+    int32_t *par, *aligned, *ind, *rank, *in_head, *in_tail, *out_head, *out_tail, *in_cnt, *out_cnt;
+    int32_t *e_from, *e_to, *e_w, *e_nin, *e_nout;
+    int32_t *rank_to_id, *hlen, *tlen, *deg, *stk, *pre, *score;
+    int32_t NC, EC;
+};
+
+__device__ DevGraph slot_graph(char* s, const SlotLayout& L) {
+    DevGraph g;
+    g.hdr = (int32_t*)(s + L.hdr);
+    g.base = (uint8_t*)(s + L.base);
+    g.par = (int32_t*)(s + L.par); g.aligned = (int32_t*)(s + L.aligned); g.ind = (int32_t*)(s + L.ind);
+    g.rank = (int32_t*)(s + L.rank);
+    g.in_head = (int32_t*)(s + L.in_head); g.in_tail = (int32_t*)(s + L.in_tail);
+    g.out_head = (int32_t*)(s + L.out_head); g.out_tail = (int32_t*)(s + L.out_tail);
+    g.in_cnt = (int32_t*)(s + L.in_cnt); g.out_cnt = (int32_t*)(s + L.out_cnt);
+    g.e_from = (int32_t*)(s + L.e_from); g.e_to = (int32_t*)(s + L.e_to); g.e_w = (int32_t*)(s + L.e_w);
+    g.e_nin = (int32_t*)(s + L.e_nin); g.e_nout = (int32_t*)(s + L.e_nout);
+    g.rank_to_id = (int32_t*)(s + L.rank_to_id); g.hlen = (int32_t*)(s + L.hlen); g.tlen = (int32_t*)(s + L.tlen);
+    g.deg = (int32_t*)(s + L.deg); g.stk = (int32_t*)(s + L.stk); g.pre = (int32_t*)(s + L.pre);
+    g.score = (int32_t*)(s + L.score);
+    g.NC = L.NC; g.EC = L.EC;
+    return g;
+}
+
+__device__ __forceinline__ uint8_t nt4_dev(uint8_t c) {
+    switch (c) {
+        case 0: case 1: case 2: case 3: return c;
+        case 'A': case 'a': return 0;
+        case 'C': case 'c': return 1;
+        case 'G': case 'g': return 2;
+        case 'T': case 't': case 'U': case 'u': return 3;
+        default: return 4;
+    }
+}
+
+// node_t ctor (include/node.h:16-22); -1 when the slot is full
+__device__ int dg_add_node(DevGraph& g, int& nn, uint8_t base) {
+    if (nn >= g.NC) return -1;
+    const int id = nn++;
+    g.base[id] = base;
+    g.par[id] = id;
+#pragma unroll
+    for (int k = 0; k < 5; k++) g.aligned[id * 5 + k] = -1;
+    g.aligned[id * 5 + base] = id;
+    g.ind[id] = 0;
+    g.in_head[id] = g.in_tail[id] = g.out_head[id] = g.out_tail[id] = -1;
+    g.in_cnt[id] = g.out_cnt[id] = 0;
+    return id;
+}
+
+// graph::add_adj (src/graph.cpp:13-20, include/node.h:23-61); false when full
+__device__ bool dg_add_adj(DevGraph& g, int& ne, int u, int v) {
+    if (u == v) return true;
+    g.ind[v]++;
+    for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
+        if (g.e_to[e] == v) { g.e_w[e]++; return true; }
+    if (ne >= g.EC) return false;
+    const int e = ne++;
+    g.e_from[e] = u; g.e_to[e] = v; g.e_w[e] = 1; g.e_nin[e] = -1; g.e_nout[e] = -1;
+    if (g.out_tail[u] >= 0) g.e_nout[g.out_tail[u]] = e; else g.out_head[u] = e;
+    g.out_tail[u] = e; g.out_cnt[u]++;
+    if (g.in_tail[v] >= 0) g.e_nin[g.in_tail[v]] = e; else g.in_head[v] = e;
+    g.in_tail[v] = e; g.in_cnt[v]++;
+    return true;
+}
+
+// graph::topsort op 0 (src/graph.cpp:61-123), lane 0 only; returns #ranks
+__device__ int dg_topsort(DevGraph& g, int nn, bool with_lens) {
+    int sp = 0, nr = 0;
+    for (int i = 0; i < nn; i++) {
+        g.deg[i] = g.in_cnt[i];
+        if (g.deg[i] == 0) g.stk[sp++] = i;
+    }
+    while (sp) {
+        const int u = g.stk[--sp];
+        g.rank[u] = nr;
+        g.rank_to_id[nr++] = u;
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) {
+            const int v = g.e_to[e];
+            if (--g.deg[v] == 0) g.stk[sp++] = v;
+        }
+    }
+    if (with_lens) {
+        for (int i = 0; i < nr; i++) {
+            const int u = g.rank_to_id[i];
+            int wmax = -1, max_pre = -1;
+            for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e])
+                if (g.e_w[e] > wmax) { wmax = g.e_w[e]; max_pre = g.rank[g.e_from[e]]; }
+            if (max_pre != -1) g.hlen[g.rank[u]] = g.hlen[max_pre] + 1;
+        }
+        g.tlen[g.rank[1]] = 1;
+        for (int i = nr - 1; i >= 0; i--) {
+            const int u = g.rank_to_id[i];
+            int wmax = -1, max_suc = -1;
+            for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
+                if (g.e_w[e] > wmax) { wmax = g.e_w[e]; max_suc = g.rank[g.e_to[e]]; }
+            if (max_suc != -1) g.tlen[g.rank[u]] = g.tlen[max_suc] + 1;
+        }
+    }
+    return nr;
+}
+
+// graph::build_consensus (src/graph.cpp:294-351), lane 0; returns its length
+// (or -1 when it does not fit into cap) and writes ASCII to out
+__device__ int dg_consensus(DevGraph& g, int nn, char* out, int cap) {
+    int qh = 0, qt = 0;
+    for (int i = 0; i < nn; i++) { g.deg[i] = g.in_cnt[i]; g.pre[i] = 0; g.score[i] = 0; }
+    g.stk[qt++] = 0;
+    while (qh < qt) {
+        const int u = g.stk[qh++];
+        if (u != 0) {
+            int wmax = -1, max_pre = -1;
+            for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e]) {
+                const int pr = g.e_from[e], wk = g.e_w[e];
+                if (wk > wmax || (wk == wmax && g.score[pr] > g.score[max_pre])) { wmax = wk; max_pre = pr; }
+            }
+            g.pre[u] = max_pre;
+            g.score[u] = g.score[max_pre] + wmax;
+        }
+        if (u == 1) break;
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
+            if (--g.deg[g.e_to[e]] == 0) g.stk[qt++] = g.e_to[e];
+    }
+    int len = 0;
+    for (int id = g.pre[1]; id != 0; id = g.pre[id]) len++;
+    if (len > cap) return -1;
+    const char nt[5] = {'A', 'C', 'G', 'T', 'N'};
+    int k = len;
+    for (int id = g.pre[1]; id != 0; id = g.pre[id]) out[--k] = nt[g.base[id]];
+    return len;
+}
+
+// Build the DP rows of window [rank(source), rank(sink)] with the whole warp.
+__device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v, int lane) {
+    const int beg_i = g.rank[0], end_i = g.rank[1];
+    const int n = end_i - beg_i + 1;
+    int32_t* in_ptr = (int32_t*)(s + L.v_in_ptr);
+    int32_t* out_ptr = (int32_t*)(s + L.v_out_ptr);
+    int32_t* in_row = (int32_t*)(s + L.v_in_row);
+    int32_t* in_w = (int32_t*)(s + L.v_in_w);
+    uint8_t* in_base = (uint8_t*)(s + L.v_in_base);
+    int32_t* out_row = (int32_t*)(s + L.v_out_row);
+    uint8_t* vb = (uint8_t*)(s + L.v_base);
+    int32_t* vind = (int32_t*)(s + L.v_ind);
+    int32_t* hq = (int32_t*)(s + L.v_hq);
+    int32_t* hq_loc = (int32_t*)(s + L.v_hq_loc);
+    int32_t* tq = (int32_t*)(s + L.v_tq);
+    const int h0 = g.hlen[beg_i], t0 = g.tlen[end_i];
+    // pass 1: per-row counts and scalars
+    for (int r = lane; r < n; r += 32) {
+        const int u = g.rank_to_id[beg_i + r];
+        int ci = 0, co = 0;
+        for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e]) ci += (g.rank[g.e_from[e]] - beg_i >= 0);
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) co += (g.rank[g.e_to[e]] - beg_i < n);
+        in_ptr[r + 1] = ci;
+        out_ptr[r + 1] = co;
+        vb[r] = g.base[u];
+        vind[r] = g.ind[u];
+        hq[r] = g.hlen[beg_i + r] - h0;
+        hq_loc[r] = g.hlen[r] - h0;
+        tq[r] = g.tlen[beg_i + r] - t0;
+    }
+    __syncwarp();
+    // exclusive scans of the counts
+    int ci_carry = 0, co_carry = 0;
+    if (lane == 0) { in_ptr[0] = 0; out_ptr[0] = 0; }
+    for (int c0 = 0; c0 < n; c0 += 32) {
+        const int r = c0 + lane;
+        int ci = r < n ? in_ptr[r + 1] : 0, co = r < n ? out_ptr[r + 1] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int yi = __shfl_up_sync(0xffffffffu, ci, o), yo = __shfl_up_sync(0xffffffffu, co, o);
+            if (lane >= o) { ci += yi; co += yo; }
+        }
+        __syncwarp();
+        if (r < n) { in_ptr[r + 1] = ci + ci_carry; out_ptr[r + 1] = co + co_carry; }
+        ci_carry += __shfl_sync(0xffffffffu, ci, 31);
+        co_carry += __shfl_sync(0xffffffffu, co, 31);
+    }
+    __syncwarp();
+    // pass 2: fill the lists in in-list / out-list order
+    for (int r = lane; r < n; r += 32) {
+        const int u = g.rank_to_id[beg_i + r];
+        int k = in_ptr[r];
+        for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e]) {
+            const int p = g.rank[g.e_from[e]] - beg_i;
+            if (p < 0) continue;
+            in_row[k] = p;
+            in_w[k] = g.e_w[e];
+            in_base[k] = p == 0 ? 4 : g.base[g.e_from[e]];
+            k++;
+        }
+        k = out_ptr[r];
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) {
+            const int sr = g.rank[g.e_to[e]] - beg_i;
+            if (sr >= n) continue;
+            out_row[k++] = sr;
+        }
+    }
+    __syncwarp();
+    v.n = n;
+    v.in_ptr = in_ptr; v.in_row = in_row; v.in_w = in_w; v.in_base = in_base;
+    v.base = vb; v.ind = vind; v.hq = hq; v.hq_loc = hq_loc; v.tq = tq;
+    v.out_ptr = out_ptr; v.out_row = out_row;
+    return beg_i;
+}
+
+__device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared* sr, int w, int lane) {
+    const SlotLayout& L = A.L;
+    DevGraph g = slot_graph(s, L);
+    const int r0 = A.win_off[w], r1 = A.win_off[w + 1];
+    const bool lens = A.f > 0;
+    int status = ST_OK;
+    int64_t cells = 0;
+    for (int x = lane; x < L.NC; x += 32) { g.hlen[x] = 0; g.tlen[x] = 0; }
+    if (lane == 0) {
+        int nn = 0;
+        dg_add_node(g, nn, 4);
+        dg_add_node(g, nn, 4);
+        g.hdr[0] = nn;
+        g.hdr[1] = 0;
+    }
+    __syncwarp();
+    WarpGroup grp{sr};
+    for (int r = r0; r < r1 && status == ST_OK; r++) {
+        const uint8_t* rd = A.seq + A.read_off[r];
+        const int len = A.read_len[r];
+        if (len > L.QC) { status = ST_CAPACITY; break; }
+        const int nn0 = g.hdr[0];
+        if (nn0 <= 2) {  // src/align.cpp:1747-1753: source + one new node per base
+            if (lane == 0) {
+                int nn = nn0, ne = g.hdr[1], anchored = 0, st = ST_OK;
+                for (int j = 0; j < len && st == ST_OK; j++) {
+                    const int cur = dg_add_node(g, nn, nt4_dev(rd[j]));
+                    if (cur < 0 || !dg_add_adj(g, ne, anchored, cur)) st = ST_CAPACITY;
+                    anchored = cur;
+                }
+                if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
+                g.hdr[0] = nn;
+                g.hdr[1] = ne;
+                if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
+                g.hdr[2] = st;
+            }
+            __syncwarp();
+            status = g.hdr[2];
+            continue;
+        }
+        // DP rows of the whole graph and the shifted query
+        WinView v;
+        const int beg_i = build_view(g, s, L, v, lane);
+        uint8_t* qs = (uint8_t*)(s + L.qs);
+        const int64_t qsb = qs_bytes(len);
+        for (int64_t x = lane; x < qsb; x += 32) qs[x] = (x >= 2 && x < len + 2) ? nt4_dev(rd[x - 2]) : 4;
+        if (lane == 0) {
+            a.v = v;
+            a.qs = qs;
+            a.qlen = len;
+            a.ab_band = A.ab_band;
+            a.f = A.f;
+            a.w = A.b + (A.f ? (len + 1) / A.f : 0);
+            a.sc = A.sc;
+            a.meta = (RowMeta*)(s + L.meta);
+            a.state = (int32_t*)(s + L.state);
+            a.rs = (int32_t*)(s + L.rs);
+            a.rs_cap = L.rs_cap;
+            a.ring_rows = L.ring_rows;
+            a.ring_blocks = L.ring_blocks;
+            a.tb = (uint8_t*)(s + L.tb);
+            a.tb_cap = L.tb_cap;
+            a.moves = (int32_t*)(s + L.moves);
+            a.moves_cap = L.NC + L.QC + 16;
+            a.out = g.hdr + 4;
+        }
+        __syncwarp();
+        if (v.n > L.NC) { status = ST_CAPACITY; break; }
+        dp_fill(grp, a);
+        __syncwarp();
+        if (lane == 0) {
+            int st = a.out[0];
+            cells += a.out[3];
+            int32_t nm = 0;
+            if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
+            if (st == ST_OK) {
+                // moves -> path -> fusion (src/align.cpp:1606-1620, 1672-1682; src/graph.cpp:170-235)
+                int nn = g.hdr[0], ne = g.hdr[1], anchored = -1;
+                for (int t = nm - 1; t >= 0 && st == ST_OK; t--) {
+                    const int32_t mv = a.moves[t];
+                    const int kind = mv_kind(mv), qc = mv_qc(mv);
+                    int cur;
+                    if (kind == MV_INSERT) {
+                        cur = dg_add_node(g, nn, (uint8_t)qc);
+                    } else {
+                        const int pre = g.rank_to_id[beg_i + mv_row(mv)];
+                        if (kind == MV_MATCH) {
+                            cur = pre;
+                        } else {
+                            const int par = g.par[pre];
+                            cur = g.aligned[par * 5 + qc];
+                            if (cur == -1) {
+                                cur = dg_add_node(g, nn, (uint8_t)qc);
+                                if (cur >= 0) {
+                                    g.aligned[par * 5 + qc] = cur;
+                                    g.par[cur] = par;
+                                }
+                            }
+                        }
+                    }
+                    if (cur < 0) { st = ST_CAPACITY; break; }
+                    if (anchored != -1 && !dg_add_adj(g, ne, anchored, cur)) st = ST_CAPACITY;
+                    anchored = cur;
+                }
+                if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
+                g.hdr[0] = nn;
+                g.hdr[1] = ne;
+                if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
+            }
+            g.hdr[2] = st;
+        }
+        __syncwarp();
+        status = g.hdr[2];
+    }
+    if (lane == 0) {
+        int len = -1;
+        if (status == ST_OK) {
+            len = dg_consensus(g, g.hdr[0], A.cons + (int64_t)w * A.cons_stride, A.cons_stride);
+            if (len < 0) status = ST_CAPACITY;
+        }
+        A.cons_len[w] = len < 0 ? 0 : len;
+        A.status[w] = status;
+        A.cells[w] = cells;
+    }
+    __syncwarp();
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_batch(BatchArgs A) {
+    __shared__ DpArgs s_args[WARPS];
+    __shared__ RowShared s_sr[WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t slot = (int64_t)blockIdx.x * WARPS + warp;
+    char* s = A.slots + slot * A.L.bytes;
+    while (true) {
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(A.counter, 1);
+        idx = __shfl_sync(0xffffffffu, idx, 0);
+        if (idx >= A.n_windows) break;
+        process_window(A, s, s_args[warp], &s_sr[warp], A.order[idx], lane);
+    }
+}
+
+}  // namespace
+
+BatchEngine::BatchEngine(int device) : device_(device) {
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cudaStream_t s;
+    cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    stream_ = s;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    ev0_ = e0;
+    ev1_ = e1;
+}
+
+BatchEngine::~BatchEngine() {
+    cudaSetDevice(device_);
+    if (d_in_) cudaFree(d_in_);
+    if (d_out_) cudaFree(d_out_);
+    if (d_slots_) cudaFree(d_slots_);
+    if (h_out_) cudaFreeHost(h_out_);
+    if (ev0_) cudaEventDestroy((cudaEvent_t)ev0_);
+    if (ev1_) cudaEventDestroy((cudaEvent_t)ev1_);
+    if (stream_) cudaStreamDestroy((cudaStream_t)stream_);
+}
+
+void BatchEngine::ensure(void** ptr, size_t* cap, size_t bytes) {
+    if (bytes <= *cap) return;
+    if (*ptr) cuda_check(cudaFree(*ptr), "cudaFree");
+    *ptr = nullptr;
+    *cap = 0;
+    cuda_check(cudaMalloc(ptr, bytes), "cudaMalloc(batch)");
+    *cap = bytes;
+}
+
+void BatchEngine::upload(const BatchInput& in, const Params& p) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    if (p.enable_seeding || p.progressive || p.result != 0)
+        throw std::invalid_argument("batched windows support the consensus mode without -S/-p");
+    p_ = p;
+    n_windows_ = in.n_windows;
+    n_reads_ = in.n_reads;
+    max_len_ = 0;
+    max_win_bases_ = 0;
+    std::vector<int64_t> cost(n_windows_);
+    for (int r = 0; r < n_reads_; r++) max_len_ = std::max(max_len_, in.read_len[r]);
+    for (int w = 0; w < n_windows_; w++) {
+        int64_t b = 0;
+        for (int r = in.win_off[w]; r < in.win_off[w + 1]; r++) b += in.read_len[r];
+        max_win_bases_ = std::max(max_win_bases_, b);
+        cost[w] = b * (in.win_off[w + 1] - in.win_off[w] + 1);
+    }
+    order_.resize(n_windows_);
+    std::iota(order_.begin(), order_.end(), 0);
+    std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    cons_stride_ = (int32_t)((2 * (int64_t)max_len_ + 64 + 15) / 16 * 16);
+
+    off_seq_ = 0;
+    size_t o = up256((size_t)in.seq_bytes + 16);
+    off_roff_ = o; o = up256(o + 8 * (size_t)n_reads_);
+    off_rlen_ = o; o = up256(o + 4 * (size_t)n_reads_);
+    off_woff_ = o; o = up256(o + 4 * (size_t)(n_windows_ + 1));
+    off_order_ = o; o = up256(o + 4 * (size_t)n_windows_);
+    off_ctr_ = o; o = up256(o + 64);
+    ensure(&d_in_, &d_in_cap_, o);
+    cudaStream_t s = (cudaStream_t)stream_;
+    char* d = (char*)d_in_;
+    cuda_check(cudaMemcpyAsync(d + off_seq_, in.seq, (size_t)in.seq_bytes, cudaMemcpyHostToDevice, s), "H2D seq");
+    cuda_check(cudaMemcpyAsync(d + off_roff_, in.read_off, 8 * (size_t)n_reads_, cudaMemcpyHostToDevice, s), "H2D");
+    cuda_check(cudaMemcpyAsync(d + off_rlen_, in.read_len, 4 * (size_t)n_reads_, cudaMemcpyHostToDevice, s), "H2D");
+    cuda_check(cudaMemcpyAsync(d + off_woff_, in.win_off, 4 * (size_t)(n_windows_ + 1), cudaMemcpyHostToDevice, s),
+               "H2D");
+    cuda_check(cudaMemcpyAsync(d + off_order_, order_.data(), 4 * (size_t)n_windows_, cudaMemcpyHostToDevice, s),
+               "H2D");
+    stats.h2d_bytes = (int64_t)(in.seq_bytes + 12 * (int64_t)n_reads_ + 8 * (int64_t)n_windows_);
+
+    out_cons_ = 0;
+    o = up256((size_t)n_windows_ * cons_stride_);
+    out_len_ = o; o = up256(o + 4 * (size_t)n_windows_);
+    out_status_ = o; o = up256(o + 4 * (size_t)n_windows_);
+    out_cells_ = o; o = up256(o + 8 * (size_t)n_windows_);
+    out_bytes_ = o;
+    ensure(&d_out_, &d_out_cap_, o);
+    if (h_out_cap_ < o) {
+        if (h_out_) cuda_check(cudaFreeHost(h_out_), "cudaFreeHost");
+        h_out_ = nullptr;
+        cuda_check(cudaMallocHost(&h_out_, o), "cudaMallocHost");
+        h_out_cap_ = o;
+    }
+    cuda_check(cudaStreamSynchronize(s), "upload");
+}
+
+void BatchEngine::run() {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream_;
+    int sms = 0;
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attr");
+    const bool adaptive = p_.f > 0 && p_.ab_band;
+    // capacities from the data (a window beyond them reports ST_CAPACITY / ST_OOM)
+    const int64_t NC64 = std::min<int64_t>(2 + max_win_bases_, 2 + 8 * (int64_t)max_len_ + 256);
+    const int32_t NC = (int32_t)NC64;
+    const int32_t EC = 3 * NC;
+    const int32_t QC = max_len_ + 8;
+    const int m = max_len_ + 1;
+    const int wb = p_.b + (p_.f ? m / p_.f : 0);
+    int ring_blocks = p_.f > 0 ? std::min(m / BLK + 2, (2 * wb) / BLK + 4) : m / BLK + 2;
+    if (adaptive) ring_blocks = std::min(m / BLK + 2, (4 * wb) / BLK + 4);
+    ring_blocks = std::max(ring_blocks, 4);
+    const int32_t ring_rows = 32;
+    const int64_t spill_rows = std::max<int64_t>(NC / 4, 64);
+    const int64_t tb_cap = (int64_t)NC * ring_blocks * BLK * 2 + 4096;
+    SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill_rows, tb_cap, adaptive);
+    const int warps = warps_per_block;
+    const int blocks = sms * blocks_per_sm;
+    const int64_t slots = (int64_t)blocks * warps;
+    ensure(&d_slots_, &d_slots_cap_, (size_t)(slots * L.bytes));
+    stats.slots = (int32_t)slots;
+    stats.slot_bytes = L.bytes;
+
+    char* d = (char*)d_in_;
+    char* o = (char*)d_out_;
+    BatchArgs A;
+    A.seq = (const uint8_t*)(d + off_seq_);
+    A.read_off = (const int64_t*)(d + off_roff_);
+    A.read_len = (const int32_t*)(d + off_rlen_);
+    A.win_off = (const int32_t*)(d + off_woff_);
+    A.order = (const int32_t*)(d + off_order_);
+    A.counter = (int32_t*)(d + off_ctr_);
+    A.n_windows = n_windows_;
+    A.sc = scoring_of(p_);
+    A.b = p_.b;
+    A.f = p_.f;
+    A.ab_band = p_.ab_band;
+    A.slots = (char*)d_slots_;
+    A.L = L;
+    A.cons = o + out_cons_;
+    A.cons_stride = cons_stride_;
+    A.cons_len = (int32_t*)(o + out_len_);
+    A.status = (int32_t*)(o + out_status_);
+    A.cells = (int64_t*)(o + out_cells_);
+    cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
+    cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
+    if (warps == 4) k_batch<4><<<blocks, 4 * 32, 0, s>>>(A);
+    else if (warps == 8) k_batch<8><<<blocks, 8 * 32, 0, s>>>(A);
+    else if (warps == 2) k_batch<2><<<blocks, 2 * 32, 0, s>>>(A);
+    else k_batch<1><<<blocks, 32, 0, s>>>(A);
+    cuda_check(cudaGetLastError(), "k_batch launch");
+    cuda_check(cudaEventRecord((cudaEvent_t)ev1_, s), "event");
+    cuda_check(cudaEventSynchronize((cudaEvent_t)ev1_), "k_batch");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, (cudaEvent_t)ev0_, (cudaEvent_t)ev1_), "elapsed");
+    stats.kernel_ms = ms;
+}
+
+void BatchEngine::sync_stats() {
+    cudaStream_t s = (cudaStream_t)stream_;
+    char* h = (char*)h_out_;
+    const size_t a = out_status_, b = out_bytes_;
+    cuda_check(cudaMemcpyAsync(h + a, (char*)d_out_ + a, b - a, cudaMemcpyDeviceToHost, s), "D2H stats");
+    cuda_check(cudaStreamSynchronize(s), "D2H stats");
+    const int32_t* st = (const int32_t*)(h + out_status_);
+    const int64_t* cl = (const int64_t*)(h + out_cells_);
+    stats.cells = 0;
+    stats.failed = 0;
+    for (int w = 0; w < n_windows_; w++) {
+        stats.cells += cl[w];
+        stats.failed += st[w] != ST_OK;
+    }
+}
+
+void BatchEngine::download(std::vector<std::string>& cons, std::vector<int32_t>& status) {
+    cudaStream_t s = (cudaStream_t)stream_;
+    char* h = (char*)h_out_;
+    cuda_check(cudaMemcpyAsync(h, d_out_, out_bytes_, cudaMemcpyDeviceToHost, s), "D2H out");
+    cuda_check(cudaStreamSynchronize(s), "D2H out");
+    stats.d2h_bytes = (int64_t)out_bytes_;
+    const int32_t* ln = (const int32_t*)(h + out_len_);
+    const int32_t* st = (const int32_t*)(h + out_status_);
+    const int64_t* cl = (const int64_t*)(h + out_cells_);
+    cons.resize(n_windows_);
+    status.resize(n_windows_);
+    stats.cells = 0;
+    stats.failed = 0;
+    for (int w = 0; w < n_windows_; w++) {
+        cons[w].assign(h + out_cons_ + (size_t)w * cons_stride_, (size_t)ln[w]);
+        status[w] = st[w];
+        stats.cells += cl[w];
+        stats.failed += st[w] != ST_OK;
+    }
+}
+
+}  // namespace pb

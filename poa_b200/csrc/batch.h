@@ -1,0 +1,73 @@
+// batch.h - the batched window engine: thousands of independent POA windows
+// (one read set -> one consensus each) in one persistent launch. Each warp
+// owns a slot of device memory holding one window's graph and DP buffers
+// and runs minipoa's whole per-window loop on the device: align the read
+// (the same DP fill as the plain kernel, on a warp), fuse the path into the
+// graph, re-sort it, next read; then the heaviest-path consensus.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "driver.h"
+
+namespace pb {
+
+struct BatchInput {
+    const uint8_t* seq;       // all reads' ASCII bases back to back
+    int64_t seq_bytes;
+    const int64_t* read_off;  // [n_reads]
+    const int32_t* read_len;  // [n_reads]
+    int32_t n_reads;
+    const int32_t* win_off;   // [n_windows + 1] read ranges per window
+    int32_t n_windows;
+};
+
+struct BatchStats {
+    double kernel_ms = 0.0;   // device time of the last run() (CUDA events)
+    int64_t cells = 0;        // DP band cells of the last run
+    int64_t dp_calls = 0;
+    int32_t slots = 0;        // concurrent windows (warps) of the persistent launch
+    int64_t slot_bytes = 0;
+    int64_t h2d_bytes = 0, d2h_bytes = 0;
+    int32_t failed = 0;       // windows that ended with a non-OK status
+    int32_t retried = 0;      // windows re-run with larger capacities
+};
+
+class BatchEngine {
+  public:
+    explicit BatchEngine(int device);
+    ~BatchEngine();
+    // Copy the windows into device memory (kept resident for run()).
+    void upload(const BatchInput& in, const Params& p);
+    // Run every uploaded window on the device; device time lands in stats.
+    void run();
+    // Per-window consensus (ASCII) and status of the last run().
+    void download(std::vector<std::string>& cons, std::vector<int32_t>& status);
+    // Device-side totals only (no consensus copy): cells and failures.
+    void sync_stats();
+    BatchStats stats;
+    int32_t warps_per_block = 4;
+    int32_t blocks_per_sm = 4;
+
+  private:
+    void ensure(void** ptr, size_t* cap, size_t bytes);
+    int device_;
+    void* stream_ = nullptr;
+    void* ev0_ = nullptr;
+    void* ev1_ = nullptr;
+    Params p_;
+    int32_t n_windows_ = 0, n_reads_ = 0, max_len_ = 0, cons_stride_ = 0;
+    int64_t max_win_bases_ = 0;
+    // device buffers
+    void* d_in_ = nullptr;      size_t d_in_cap_ = 0;    // reads + offsets + window table + order
+    void* d_out_ = nullptr;     size_t d_out_cap_ = 0;   // consensus + lengths + status + cells
+    void* d_slots_ = nullptr;   size_t d_slots_cap_ = 0;
+    void* h_out_ = nullptr;     size_t h_out_cap_ = 0;   // pinned mirror of d_out_
+    size_t off_seq_ = 0, off_roff_ = 0, off_rlen_ = 0, off_woff_ = 0, off_order_ = 0, off_ctr_ = 0;
+    size_t out_cons_ = 0, out_len_ = 0, out_status_ = 0, out_cells_ = 0, out_bytes_ = 0;
+    std::vector<int32_t> order_;
+};
+
+}  // namespace pb

@@ -7,12 +7,14 @@
 #include <string>
 
 #include "../../include/poa_b200.h"
+#include "batch.h"
 #include "gpu_engine.h"
 
 struct poa_ctx {
     int device = 0;
     pb::Params p;
     pb::GpuEngine* eng = nullptr;
+    pb::BatchEngine* batch = nullptr;
     std::string err;
 };
 
@@ -139,6 +141,7 @@ poa_ctx* poa_create(int device, const poa_params* p) {
 
 void poa_destroy(poa_ctx* ctx) {
     if (!ctx) return;
+    delete ctx->batch;
     delete ctx->eng;
     delete ctx;
 }
@@ -225,6 +228,83 @@ int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* 
     } catch (const std::exception& e) {
         return fail(ctx, POA_CUDA, e.what());
     }
+}
+
+int poa_batch_upload(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                     const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows) {
+    if (!ctx || (seq_bytes > 0 && !seq) || n_reads < 0 || n_windows < 0 || (n_reads > 0 && (!read_off || !read_len)) ||
+        !win_off)
+        return fail(ctx, POA_BAD_ARG, "null argument");
+    if (win_off[0] != 0 || win_off[n_windows] != n_reads) return fail(ctx, POA_BAD_ARG, "win_off must span all reads");
+    for (int32_t w = 0; w < n_windows; w++)
+        if (win_off[w + 1] < win_off[w]) return fail(ctx, POA_BAD_ARG, "win_off must be non-decreasing");
+    for (int32_t r = 0; r < n_reads; r++)
+        if (read_len[r] < 0 || read_off[r] < 0 || read_off[r] + read_len[r] > seq_bytes)
+            return fail(ctx, POA_BAD_ARG, "read outside seq");
+    if (ctx->p.enable_seeding || ctx->p.progressive || ctx->p.result != 0)
+        return fail(ctx, POA_UNSUPPORTED, "batched windows run the consensus mode without -S/-p");
+    try {
+        if (!ctx->batch) ctx->batch = new pb::BatchEngine(ctx->device);
+        pb::BatchInput in{seq, seq_bytes, read_off, read_len, n_reads, win_off, n_windows};
+        ctx->batch->upload(in, ctx->p);
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+}
+
+int poa_batch_run(poa_ctx* ctx, double* device_ms) {
+    if (!ctx || !ctx->batch) return fail(ctx, POA_BAD_ARG, "nothing uploaded");
+    try {
+        ctx->batch->run();
+        if (device_ms) *device_ms = ctx->batch->stats.kernel_ms;
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+}
+
+int poa_batch_download(poa_ctx* ctx, char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status) {
+    if (!ctx || !ctx->batch || !cons_off || !status) return fail(ctx, POA_BAD_ARG, "null argument");
+    try {
+        std::vector<std::string> c;
+        std::vector<int32_t> st;
+        ctx->batch->download(c, st);
+        int64_t pos = 0;
+        for (size_t w = 0; w < c.size(); w++) {
+            cons_off[w] = pos;
+            if (pos + (int64_t)c[w].size() > cons_cap) return fail(ctx, POA_BAD_ARG, "consensus buffer too small");
+            if (!c[w].empty()) std::memcpy(cons + pos, c[w].data(), c[w].size());
+            pos += (int64_t)c[w].size();
+            status[w] = st[w];
+        }
+        cons_off[c.size()] = pos;
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+}
+
+int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                        const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows,
+                        char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status) {
+    int st = poa_batch_upload(ctx, seq, seq_bytes, read_off, read_len, n_reads, win_off, n_windows);
+    if (st != POA_OK) return st;
+    st = poa_batch_run(ctx, nullptr);
+    if (st != POA_OK) return st;
+    return poa_batch_download(ctx, cons, cons_cap, cons_off, status);
+}
+
+int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
+    if (!ctx || !ctx->batch || !o) return POA_BAD_ARG;
+    try {
+        ctx->batch->sync_stats();
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+    const pb::BatchStats& s = ctx->batch->stats;
+    o[0] = s.cells; o[1] = s.failed; o[2] = s.slots; o[3] = s.slot_bytes; o[4] = s.h2d_bytes; o[5] = s.d2h_bytes;
+    return POA_OK;
 }
 
 int poa_stats(const poa_ctx* ctx, int64_t* o) {

@@ -40,6 +40,12 @@ struct DpArgs {
     int32_t* state;      // [AB_NSTATE * n] when adaptive
     int32_t* rs;         // row store: M/D blocks, 16 int32 per block
     int64_t rs_cap;      // int32 units
+    // Row store layout. With ring_rows > 0 the first ring_rows * ring_blocks * 16
+    // int32 are a ring of recent rows (row i in slot i % ring_rows). A row goes
+    // to the spill area after the ring (bump-allocated) instead when one of its
+    // in-window successors is ring_rows or more rows ahead, or when it is wider
+    // than ring_blocks. ring_rows == 0 stores every row linearly.
+    int32_t ring_rows, ring_blocks;
     uint8_t* tb;         // traceback records
     int64_t tb_cap;      // bytes
     int32_t* moves;      // backtrack moves (reverse order)
@@ -48,7 +54,7 @@ struct DpArgs {
 };
 
 // Size of the shifted query buffer for a query of qlen bases.
-inline int64_t qs_bytes(int32_t qlen) {
+PB_HD int64_t qs_bytes(int32_t qlen) {
     int64_t m = (int64_t)qlen + 1;
     int64_t need = (m / BLK + 3) * BLK;
     return (need + 15) / 16 * 16;

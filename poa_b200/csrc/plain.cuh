@@ -72,17 +72,99 @@ __device__ __forceinline__ int64_t align16(int64_t x) { return (x + 15) & ~(int6
 struct RowShared {
     int32_t Bs, Be, bn, e0, d, status;
     int64_t st, tb;
-    int64_t st_next, tb_next;
+    int64_t st_next, tb_next;  // next free row-store offset (spill area when ringed), next record offset
 };
 
+// A thread group that fills one alignment: the whole CTA (plain kernel) ...
 template <int NT>
-__device__ void dp_fill_cta(const DpArgs& a) {
-    constexpr int NW = NT / 32;
-    __shared__ int32_t s_scan[NW], s_scan2[NW], s_lastM[NW], s_lastI[NW];
-    __shared__ unsigned long long s_key[NW];
-    __shared__ RowShared sr;
+struct CtaGroup {
+    static constexpr int SIZE = NT;
+    static constexpr int NW = NT / 32;
+    int32_t* s_scan;
+    int32_t* s_scan2;
+    int32_t* s_lastM;
+    int32_t* s_lastI;
+    unsigned long long* s_key;
+    RowShared* sr;
+    __device__ __forceinline__ int tid() const { return threadIdx.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    // exclusive prefix max of per-thread aggregates; total = max over the group
+    __device__ __forceinline__ int32_t excl_max(int32_t agg, int32_t& total) const {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const int32_t incl = warp_incl_max(agg);
+        int32_t ex_w = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex_w = INT_MIN;
+        if (lane == 31) s_scan[wid] = incl;
+        __syncthreads();
+        if (wid == 0) {
+            int32_t v = lane < NW ? s_scan[lane] : INT_MIN;
+            v = warp_incl_max(v);
+            if (lane < NW) s_scan2[lane] = v;
+        }
+        __syncthreads();
+        total = s_scan2[NW - 1];
+        return mx(ex_w, wid > 0 ? s_scan2[wid - 1] : INT_MIN);
+    }
+    // left neighbour (M, I of the previous thread's last cell) and the values
+    // of the group's last thread (the carry into the next chunk)
+    __device__ __forceinline__ void edges(int32_t m7, int32_t i7, int32_t carryM, int32_t carryI, int32_t& Ml0,
+                                          int32_t& Il0, int32_t& nextM, int32_t& nextI) const {
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const int32_t upM = __shfl_up_sync(0xffffffffu, m7, 1);
+        const int32_t upI = __shfl_up_sync(0xffffffffu, i7, 1);
+        if (lane == 31) { s_lastM[wid] = m7; s_lastI[wid] = i7; }
+        __syncthreads();
+        Ml0 = lane > 0 ? upM : (wid > 0 ? s_lastM[wid - 1] : carryM);
+        Il0 = lane > 0 ? upI : (wid > 0 ? s_lastI[wid - 1] : carryI);
+        nextM = s_lastM[NW - 1];
+        nextI = s_lastI[NW - 1];
+    }
+    __device__ __forceinline__ unsigned long long max_u64(unsigned long long v) const {
+        v = warp_max_u64(v);
+        if ((threadIdx.x & 31) == 0) s_key[threadIdx.x >> 5] = v;
+        __syncthreads();
+        unsigned long long k = 0ull;
+        for (int w = 0; w < NW; w++) k = s_key[w] > k ? s_key[w] : k;
+        return k;
+    }
+    // thread 0 wrote *sr; make it visible to the group
+    __device__ __forceinline__ void publish() const { __syncthreads(); }
+};
 
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+// ... or one warp (batched kernel: one warp per window)
+struct WarpGroup {
+    static constexpr int SIZE = 32;
+    RowShared* sr;
+    __device__ __forceinline__ int tid() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    __device__ __forceinline__ int32_t excl_max(int32_t agg, int32_t& total) const {
+        const int lane = threadIdx.x & 31;
+        const int32_t incl = warp_incl_max(agg);
+        int32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = INT_MIN;
+        total = __shfl_sync(0xffffffffu, incl, 31);
+        return ex;
+    }
+    __device__ __forceinline__ void edges(int32_t m7, int32_t i7, int32_t carryM, int32_t carryI, int32_t& Ml0,
+                                          int32_t& Il0, int32_t& nextM, int32_t& nextI) const {
+        const int lane = threadIdx.x & 31;
+        const int32_t upM = __shfl_up_sync(0xffffffffu, m7, 1);
+        const int32_t upI = __shfl_up_sync(0xffffffffu, i7, 1);
+        Ml0 = lane > 0 ? upM : carryM;
+        Il0 = lane > 0 ? upI : carryI;
+        nextM = __shfl_sync(0xffffffffu, m7, 31);
+        nextI = __shfl_sync(0xffffffffu, i7, 31);
+    }
+    __device__ __forceinline__ unsigned long long max_u64(unsigned long long v) const { return warp_max_u64(v); }
+    __device__ __forceinline__ void publish() const { __syncwarp(); }
+};
+
+// Fill all rows of one alignment with group G (see the file comment).
+template <class G>
+__device__ void dp_fill(const G& g, const DpArgs& a) {
+    constexpr int NT = G::SIZE;
+    RowShared& sr = *g.sr;
+    const int tid = g.tid();
     const int n = a.v.n, m = a.qlen + 1;
     const bool adaptive = a.f > 0 && a.ab_band;
     const Scoring sc = a.sc;
@@ -90,10 +172,10 @@ __device__ void dp_fill_cta(const DpArgs& a) {
     if (adaptive)
         for (int r = tid; r < n; r += NT) adaptive_init_entry(a, r, m);
     if (tid == 0) {
-        sr.st_next = 0;
+        sr.st_next = a.ring_rows > 0 ? (int64_t)a.ring_rows * a.ring_blocks * 16 : 0;
         sr.tb_next = 0;
     }
-    __syncthreads();
+    g.sync();
 
     int64_t cells = 0;
     for (int i = 0; i < n; i++) {
@@ -106,12 +188,24 @@ __device__ void dp_fill_cta(const DpArgs& a) {
             const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
             int st = ST_OK;
             const int bpc = d >= 2 ? 4 : 1;
+            int64_t row_st = sr.st_next;
+            bool linear = true;
+            if (a.ring_rows > 0) {
+                int maxs = i;
+                for (int e = a.v.out_ptr[i]; e < a.v.out_ptr[i + 1]; e++) maxs = max(maxs, a.v.out_row[e]);
+                const bool spill = (maxs - i >= a.ring_rows) || (bn > a.ring_blocks);
+                if (!spill) {
+                    row_st = (int64_t)(i % a.ring_rows) * a.ring_blocks * 16;
+                    linear = false;
+                }
+            }
             if (bn < 0) st = ST_DEGENERATE;
             else if (d > MAX_MULTI_PRED) st = ST_INDEGREE;
-            else if (sr.st_next + (int64_t)bn * 16 > a.rs_cap || sr.tb_next + (int64_t)bn * BLK * bpc > a.tb_cap)
+            else if ((linear && row_st + (int64_t)bn * 16 > a.rs_cap) || sr.tb_next + (int64_t)bn * BLK * bpc > a.tb_cap)
                 st = ST_OOM;
+            if (linear) sr.st_next = row_st + (int64_t)bn * 16;
             sr.Bs = Bs; sr.Be = Be; sr.bn = bn; sr.e0 = e0; sr.d = d; sr.status = st;
-            sr.st = sr.st_next;
+            sr.st = row_st;
             sr.tb = sr.tb_next;
             if (st == ST_OK) {
                 RowMeta rm;
@@ -119,7 +213,7 @@ __device__ void dp_fill_cta(const DpArgs& a) {
                 a.meta[i] = rm;
             }
         }
-        __syncthreads();
+        g.publish();
         const int Bs = sr.Bs, bn = sr.bn, e0 = sr.e0, d = sr.d;
         const int64_t rst = sr.st, rtb = sr.tb;
         if (sr.status != ST_OK) {
@@ -179,21 +273,9 @@ __device__ void dp_fill_cta(const DpArgs& a) {
                 H0[l] = mx(Mpre[l], Dv[l]);
                 if (act) agg = mx(agg, scan_key(H0[l], b * BLK + l, sc.e1));
             }
-            // CTA exclusive prefix max of the per-thread aggregates
-            const int32_t incl = warp_incl_max(agg);
-            int32_t ex_w = __shfl_up_sync(0xffffffffu, incl, 1);
-            if (lane == 0) ex_w = INT_MIN;
-            if (lane == 31) s_scan[wid] = incl;
-            __syncthreads();
-            if (wid == 0) {
-                int32_t v = lane < NW ? s_scan[lane] : INT_MIN;
-                v = warp_incl_max(v);
-                if (lane < NW) s_scan2[lane] = v;
-            }
-            __syncthreads();
-            const int32_t ex_b = wid > 0 ? s_scan2[wid - 1] : INT_MIN;
-            const int32_t chunk_total = s_scan2[NW - 1];
-            int32_t P = mx(ex_w, ex_b);
+            // group exclusive prefix max of the per-thread aggregates
+            int32_t chunk_total;
+            int32_t P = g.excl_max(agg, chunk_total);
             if (haveP) P = mx(P, carryP);
             if (act) {
                 if (i == 0) {
@@ -207,13 +289,8 @@ __device__ void dp_fill_cta(const DpArgs& a) {
                 for (int l = 0; l < BLK; l++) { M[l] = NEG_INF; I[l] = NEG_INF; }
             }
             // left neighbours of lane 0 of the block
-            const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
-            const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
-            if (lane == 31) { s_lastM[wid] = M[BLK - 1]; s_lastI[wid] = I[BLK - 1]; }
-            __syncthreads();
-            const int32_t Ml0 = lane > 0 ? upM : (wid > 0 ? s_lastM[wid - 1] : carryM);
-            const int32_t Il0 = lane > 0 ? upI : (wid > 0 ? s_lastI[wid - 1] : carryI);
-            const int32_t nextM = s_lastM[NW - 1], nextI = s_lastI[NW - 1];
+            int32_t Ml0, Il0, nextM, nextI;
+            g.edges(M[BLK - 1], I[BLK - 1], carryM, carryI, Ml0, Il0, nextM, nextI);
             if (act) {
                 FlagAcc acc;
                 flag_acc_init(acc);
@@ -275,22 +352,17 @@ __device__ void dp_fill_cta(const DpArgs& a) {
             carryI = nextI;
         }
         if (adaptive && i >= 1) {
-            best = warp_max_u64(best);
-            if (lane == 0) s_key[wid] = best;
-            __syncthreads();
+            const unsigned long long k = g.max_u64(best);
             if (tid == 0) {
-                unsigned long long k = 0ull;
-                for (int w = 0; w < NW; w++) k = s_key[w] > k ? s_key[w] : k;
                 const int max_j = bn > 0 ? (int)(0xffffffffu - (uint32_t)(k & 0xffffffffu)) : 0;
                 adaptive_update(a, i, Bs, max_j);
             }
         }
         if (tid == 0) {
             const int bpc = d >= 2 ? 4 : 1;
-            sr.st_next = rst + (int64_t)bn * 16;
             sr.tb_next = align16(rtb + (int64_t)bn * BLK * bpc);
         }
-        __syncthreads();
+        g.sync();
     }
     if (tid == 0) {
         const RowMeta last = a.meta[n - 1];
@@ -312,7 +384,12 @@ __global__ void __launch_bounds__(NT, 1) k_plain(const DpArgs* __restrict__ jobs
         if (threadIdx.x == 0) a.out[0] = ST_BAD_ARG;
         return;
     }
-    dp_fill_cta<NT>(a);
+    constexpr int NW = NT / 32;
+    __shared__ int32_t s_scan[NW], s_scan2[NW], s_lastM[NW], s_lastI[NW];
+    __shared__ unsigned long long s_key[NW];
+    __shared__ RowShared sr;
+    CtaGroup<NT> g{s_scan, s_scan2, s_lastM, s_lastI, s_key, &sr};
+    dp_fill(g, a);
     __syncthreads();
     if (threadIdx.x == 0 && a.out[0] == ST_OK) {
         int32_t nm = 0;

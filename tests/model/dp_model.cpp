@@ -62,6 +62,9 @@ struct ModelEngine : DpEngine {
         tb.assign((size_t)(n * (full_blocks * BLK * 4 + 16) + 16), 0);
         a.rs = rs.data();
         a.rs_cap = (int64_t)rs.size();
+        // a small ring (4 rows) exercises the ring/spill placement of the kernels
+        a.ring_rows = 4;
+        a.ring_blocks = (int32_t)std::min<int64_t>(full_blocks, 24);
         a.tb = tb.data();
         a.tb_cap = (int64_t)tb.size();
         fill(a, m);
@@ -81,7 +84,8 @@ struct ModelEngine : DpEngine {
         const bool adaptive = a.f > 0 && a.ab_band;
         if (adaptive)
             for (int r = 0; r < n; r++) adaptive_init_entry(a, r, m);
-        int64_t st_next = 0, tb_next = 0, cells = 0;
+        int64_t st_next = a.ring_rows > 0 ? (int64_t)a.ring_rows * a.ring_blocks * 16 : 0;
+        int64_t tb_next = 0, cells = 0;
         std::vector<int32_t> H0, Dk, Mf, If;
         for (int i = 0; i < n; i++) {
             int Bs, Be;
@@ -92,11 +96,22 @@ struct ModelEngine : DpEngine {
             const int e0 = a.v.in_ptr[i], d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
             if (d > MAX_MULTI_PRED) { a.out[0] = ST_INDEGREE; return; }
             const int bpc = d >= 2 ? 4 : 1;
-            RowMeta rm{Bs, Be, st_next, tb_next};
-            if (st_next + (int64_t)bn * 16 > a.rs_cap || tb_next + (int64_t)bn * BLK * bpc > a.tb_cap) {
+            int64_t row_st = st_next;
+            bool linear = true;
+            if (a.ring_rows > 0) {
+                int maxs = i;
+                for (int e = a.v.out_ptr[i]; e < a.v.out_ptr[i + 1]; e++) maxs = std::max(maxs, a.v.out_row[e]);
+                if (!((maxs - i >= a.ring_rows) || (bn > a.ring_blocks))) {
+                    row_st = (int64_t)(i % a.ring_rows) * a.ring_blocks * 16;
+                    linear = false;
+                }
+            }
+            RowMeta rm{Bs, Be, row_st, tb_next};
+            if ((linear && row_st + (int64_t)bn * 16 > a.rs_cap) || tb_next + (int64_t)bn * BLK * bpc > a.tb_cap) {
                 a.out[0] = ST_OOM;
                 return;
             }
+            if (linear) st_next = row_st + (int64_t)bn * 16;
             a.meta[i] = rm;
             cells += (int64_t)bn * BLK;
             H0.assign((size_t)bn * BLK, 0);
@@ -174,7 +189,6 @@ struct ModelEngine : DpEngine {
                 for (int j = 1; j < bn * BLK; j++) max_j = Mf[j] > Mf[max_j] ? j : max_j;
                 adaptive_update(a, i, Bs, max_j);
             }
-            st_next += (int64_t)bn * 16;
             tb_next = align16(tb_next + (int64_t)bn * BLK * bpc);
         }
         const RowMeta last = a.meta[n - 1];

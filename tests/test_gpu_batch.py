@@ -1,0 +1,86 @@
+"""Batched window engine (graph fusion, topsort and consensus on the device)
+against the reference: every window's consensus must equal minipoa's output
+on that window's reads."""
+import json
+import os
+import subprocess
+
+import pytest
+
+import poa_b200
+from poa_b200 import synth
+from tests import fasta
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden")
+with open(os.path.join(GOLD, "manifest.json")) as fh:
+    MANIFEST = {c["case"]: c for c in json.load(fh)}
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden_windows(names):
+    reads, offs = [], [0]
+    for nm in names:
+        _, seqs = fasta.read(os.path.join(GOLD, nm + ".fa"))
+        reads.extend(seqs)
+        offs.append(offs[-1] + len(seqs))
+    return synth.pack_windows_from_reads(reads, offs)
+
+
+def _cons_of(out_text):
+    lines = out_text.split(b"\n")
+    return lines[1] if len(lines) > 1 else b""
+
+
+def _check(names, opts, upload_path=True):
+    ws = _golden_windows(names)
+    with poa_b200.Context(poa_b200.Params.from_cli(opts)) as ctx:
+        if upload_path:
+            ctx.batch_upload(ws)
+            ctx.batch_run()
+            cons, st = ctx.batch_download()
+        else:
+            cons, st = ctx.batch_consensus(ws)
+    for w, nm in enumerate(names):
+        want = _cons_of(open(os.path.join(GOLD, nm + ".out"), "rb").read())
+        assert st[w] == 0, (nm, st[w])
+        assert cons[w] == want, nm
+
+
+def test_batch_golden_windows():
+    _check([f"window_{w:02d}" for w in range(10)], [])
+
+
+def test_batch_golden_windows_e2e_entry():
+    _check([f"window_{w:02d}" for w in range(10)], [], upload_path=False)
+
+
+def test_batch_golden_adaptive():
+    _check([f"lbwindow_{w:02d}" for w in range(3)] + ["noisy_adaptive"], ["-B"])
+
+
+def test_batch_golden_edges():
+    _check(["edge_mixed", "edge_single", "edge_empty_read", "edge_all_n", "edge_identical", "cons_small"], [])
+
+
+def test_batch_golden_scoring():
+    _check(["cons_scoring"], MANIFEST["cons_scoring"]["opts"])
+
+
+def test_batch_vs_oracle(oracle_bin, tmp_path):
+    ws = synth.polishing_windows(seed=31, n_windows=40)
+    with poa_b200.Context() as ctx:
+        ctx.batch_upload(ws)
+        ctx.batch_run()
+        cons, st = ctx.batch_download()
+        # a second run on the resident inputs must give the same answer
+        ctx.batch_run()
+        cons2, st2 = ctx.batch_download()
+    assert cons == cons2 and st == st2
+    for w in range(ws.n_windows):
+        fa = tmp_path / f"w{w}.fa"
+        synth.write_fasta(str(fa), ws.window_reads(w))
+        want = subprocess.run([oracle_bin, str(fa)], capture_output=True, check=True).stdout
+        assert st[w] == 0
+        assert cons[w] == _cons_of(want), w

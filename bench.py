@@ -1,0 +1,362 @@
+"""Benchmark: batched POA polishing windows on B200.
+
+Workload (one step): 20,000 independent polishing windows (template
+500 +- 100 bp, 4-64 reads, 8 % error split 4:3:3 into substitutions,
+insertions and deletions; seeded synthetic data), each aligned progressively
+into its own POA graph in minipoa's default consensus mode (static band
+b=100, f=40, scoring 2/-4/-4/-2); output one consensus per window,
+bit-exact with minipoa.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value  windows/s over all ranks with the inputs resident in HBM (device time
+       of the persistent batch kernel, CUDA events on its stream).
+e2e    windows/s through the public C ABI (poa_batch_consensus) with the
+       inputs in pinned host memory: upload, kernel, consensus download.
+Multi-GPU: every rank runs its own 20,000 windows (weak scaling, no
+collective on the data path; torch.distributed only for the barrier and the
+max over ranks of the time).
+``--impl reference`` times the reference's own CPU build (oracle/_ref/minipoa,
+compiled from the reference sources) on a bounded sample of the same
+windows with every host core, one process per window.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "windows/s & GCUPS on 1 B200: learned-band+batched vs plain kernel, bit-exact"
+WORKLOAD = "polishing_windows: 20000 windows, template 500+-100 bp, 4-64 reads, 8% error (4:3:3), consensus"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "minipoa")
+PORT_BIN = os.path.join(ROOT, "oracle", "build", "poa_oracle")
+# algorithmic work per DP cell: 1 byte of traceback record written
+# (SURVEY-style unit: cell = one computed band cell, (Be-Bs-1)*8 per row)
+BYTES_PER_CELL = 1.0
+# int32 operations per cell and per edge-cell of the recurrence
+OPS_PER_CELL, OPS_PER_EDGE_CELL = 5, 7
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rk = int(os.environ.get("RANK", "0"))
+    lr = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rk, lr
+
+
+class Dist:
+    def __init__(self, world):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            if torch.cuda.is_available():
+                t = torch.ones(1, device="cuda")
+                self.pg.all_reduce(t)
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", gpu_id, "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def gpu_uuid(dev: int) -> str:
+    try:
+        import torch
+        u = torch.cuda.get_device_properties(dev).uuid
+        return "GPU-" + str(u)
+    except Exception:
+        return str(dev)
+
+
+def load_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": d.get("hbm_gbs"), "src": "measured", "sm_max_mhz": d.get("sm_max_mhz", 1965.0)}
+    return {"hbm_gbs": 6650.0, "src": "fallback", "sm_max_mhz": 1965.0}
+
+
+def profile_traffic_per_cell():
+    """DRAM bytes per DP cell of k_batch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_batch_dram.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    return d.get("dram_bytes_per_cell")
+
+
+# --------------------------------------------------------------------- CPU leg
+def write_windows(ws, idx, d):
+    from poa_b200 import synth
+    paths = []
+    for w in idx:
+        fa = os.path.join(d, f"w{w}.fa")
+        synth.write_fasta(fa, ws.window_reads(int(w)))
+        paths.append(fa)
+    return paths
+
+
+def run_cpu_windows(binary, paths, cores):
+    def one(fa):
+        return subprocess.run([binary, fa], capture_output=True, check=True).stdout
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        return list(ex.map(one, paths))
+
+
+def cpu_sample(ws, seconds, cores, binary):
+    """Windows/s of the CPU binary on windows 0.. of ws, about `seconds` of work."""
+    with tempfile.TemporaryDirectory() as d:
+        probe = write_windows(ws, range(min(cores, ws.n_windows)), d)
+        t0 = time.perf_counter()
+        run_cpu_windows(binary, probe, cores)
+        per = (time.perf_counter() - t0) / max(len(probe), 1) * cores  # seconds per window per core
+        n = int(min(ws.n_windows, max(cores, seconds * cores / max(per, 1e-3))))
+        paths = write_windows(ws, range(n), d)
+        t0 = time.perf_counter()
+        outs = run_cpu_windows(binary, paths, cores)
+        dt = time.perf_counter() - t0
+    return n / dt, n, dt, outs
+
+
+# --------------------------------------------------------------------- arms
+def ours(args, world, rank, local, D):
+    import poa_b200
+    from poa_b200 import synth
+    t0 = time.perf_counter()
+    ws = synth.polishing_windows(seed=4 + 1000 * rank, n_windows=args.windows)
+    log(f"[rank {rank}] generated {ws.n_windows} windows / {ws.n_reads} reads in {time.perf_counter() - t0:.1f}s")
+    try:
+        import torch
+        torch.cuda.set_device(local)
+    except Exception:
+        pass
+    ctx = poa_b200.Context(poa_b200.Params(), device=local)
+
+    # ---- device-resident leg
+    ctx.batch_upload(ws)
+    for _ in range(args.warmup):
+        ctx.batch_run()
+    D.barrier()
+    clk = ClockSampler(gpu_uuid(local))
+    dev_ms = []
+    for _ in range(args.steps):
+        dev_ms.append(ctx.batch_run())
+    D.barrier()
+    clocks = clk.stop()
+    st = ctx.batch_stats()
+    t_dev = D.max(sum(dev_ms) / 1e3)
+    cells = st["cells"]
+    failed = int(D.sum(st["failed"]))
+    cons, status = ctx.batch_download()
+
+    # ---- end-to-end leg through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        holders = []
+        arrs = []
+        for a in (ws.seq, ws.read_off, ws.read_len, ws.win_off):
+            h, v = poa_b200.pinned_copy(np.ascontiguousarray(a))
+            holders.append(h)
+            arrs.append(v)
+        pws = synth.WindowSet(seq=arrs[0], read_off=arrs[1], read_len=arrs[2], win_off=arrs[3])
+        for _ in range(max(1, args.warmup)):
+            ctx.batch_consensus(pws)
+        D.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            c2, s2 = ctx.batch_consensus(pws)
+        D.barrier()
+        t_e2e = D.max(time.perf_counter() - t0)
+        st2 = ctx.batch_stats()
+        e2e = {"value": world * ws.n_windows * args.steps / t_e2e, "unit": "windows/s",
+               "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
+               "ms_per_step": 1e3 * t_e2e / args.steps, "api": "poa_batch_consensus"}
+        assert c2 == cons and s2 == status, "end-to-end run disagrees with the device-resident run"
+        for h in holders:
+            h.close()
+
+    value = world * ws.n_windows * args.steps / t_dev
+    kernel_s = t_dev / args.steps
+    peaks = load_peaks()
+    achieved = cells * BYTES_PER_CELL / kernel_s / 1e9
+    tpc = profile_traffic_per_cell()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_src": peaks["src"],
+                "traffic": (tpc * cells if tpc is not None else None),
+                "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL, "kernel": "k_batch"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * kernel_s, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": WORKLOAD, "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
+                   "bases_per_rank": int(ws.seq.shape[0]), "mode": "consensus, static band b=100 f=40",
+                   "parallelism": f"windows sharded over {world} GPU(s)",
+                   "l2": "inputs (%.0f MB) larger than L2 (126 MB)" % (ws.seq.shape[0] / 1e6)},
+        "gcups": world * cells * args.steps / t_dev / 1e9,
+        "cells_per_step": cells, "failed_windows": failed,
+        "gpu_launches": args.steps, "e2e": e2e, "roofline": roofline, "clocks": clocks,
+        "slots": st["slots"], "slot_bytes": st["slot_bytes"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
+        kind = "reference" if binary == REF_BIN else "port"
+        cores = len(os.sched_getaffinity(0))
+        v, n, dt, outs = cpu_sample(ws, args.cpu_seconds, cores, binary)
+        same = sum(1 for w in range(n) if outs[w] == b">consensus sequence\n" + cons[w] + b"\n")
+        line["cpu_baseline"] = {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
+                                "sample": f"first {n} of the {ws.n_windows} windows, one process per window, "
+                                          f"{dt:.1f}s wall"}
+        line["parity_sample"] = {"windows": n, "identical_consensus": same}
+    ctx.close()
+    return line
+
+
+def reference(args, world, rank, local, D):
+    from poa_b200 import synth
+    if rank != 0:
+        return None
+    binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
+    kind = "reference" if binary == REF_BIN else "port"
+    cores = len(os.sched_getaffinity(0))
+    ws = synth.polishing_windows(seed=4, n_windows=min(args.windows, args.ref_windows_per_step * cores))
+    per_step = min(ws.n_windows, args.ref_windows_per_step * cores)
+    with tempfile.TemporaryDirectory() as d:
+        paths = write_windows(ws, range(per_step), d)
+        for _ in range(args.warmup):
+            run_cpu_windows(binary, paths[:cores], cores)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            run_cpu_windows(binary, paths, cores)
+        dt = time.perf_counter() - t0
+    v = per_step * args.steps / dt
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "windows/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded; no dataset)",
+            "config": {"workload": WORKLOAD, "windows_per_step": per_step},
+            "cpu_baseline": {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
+                             "sample": f"{per_step} windows per step, one {kind} process per window, "
+                                       f"{cores} concurrent"},
+            "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--windows", type=int, default=20000)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-windows-per-step", type=int, default=40)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        line = reference(args, world, rank, local, None)
+        print(json.dumps(line), flush=True)
+        return
+    D = Dist(world)
+    try:
+        line = ours(args, world, rank, local, D)
+    finally:
+        D.close()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -133,6 +133,11 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes. */
 int poa_batch_stats(poa_ctx* ctx, int64_t* out6);
 
+/* Page-locked host memory (cudaMallocHost) for callers that want the
+ * batch copies to run at full PCIe/NVLink-C2C speed; NULL on failure. */
+void* poa_alloc_pinned(size_t bytes);
+void poa_free_pinned(void* ptr);
+
 /* Counters since poa_create: [0] kernel launches, [1] alignments, [2] band
  * cells, [3] kernel time in microseconds (when timing is on), [4] H2D bytes,
  * [5] D2H bytes. */

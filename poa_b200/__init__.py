@@ -116,6 +116,9 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, _i64p, _i32p]
     L.poa_batch_stats.argtypes = [ctypes.c_void_p, _i64p]
     L.poa_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.poa_alloc_pinned.restype = ctypes.c_void_p
+    L.poa_alloc_pinned.argtypes = [ctypes.c_size_t]
+    L.poa_free_pinned.argtypes = [ctypes.c_void_p]
     _lib = L
     return L
 
@@ -237,6 +240,34 @@ class Context:
         o = (ctypes.c_int64 * 6)()
         lib().poa_stats(self._h, o)
         return dict(launches=o[0], alignments=o[1], cells=o[2], kernel_us=o[3], h2d_bytes=o[4], d2h_bytes=o[5])
+
+
+class PinnedArray:
+    """A numpy array over page-locked host memory (released with close())."""
+
+    def __init__(self, shape, dtype):
+        import numpy as np
+        self.dtype = np.dtype(dtype)
+        n = int(np.prod(shape)) if shape else 1
+        nbytes = max(n * self.dtype.itemsize, 1)
+        self._p = lib().poa_alloc_pinned(nbytes)
+        if not self._p:
+            raise PoaError(4, "cudaMallocHost failed")
+        buf = (ctypes.c_char * nbytes).from_address(self._p)
+        self.array = np.frombuffer(buf, dtype=self.dtype, count=n).reshape(shape)
+
+    def close(self):
+        if self._p:
+            self.array = None
+            lib().poa_free_pinned(self._p)
+            self._p = None
+
+
+def pinned_copy(a):
+    """Copy a numpy array into page-locked memory; returns (holder, array)."""
+    h = PinnedArray(a.shape, a.dtype)
+    h.array[...] = a
+    return h, h.array
 
 
 def run(seqs: Sequence[bytes], params: Optional[Params] = None, headers=None, device: int = 0) -> bytes:

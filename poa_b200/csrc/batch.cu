@@ -555,7 +555,14 @@ void BatchEngine::run() {
     const int64_t tb_cap = (int64_t)NC * ring_blocks * BLK * 2 + 4096;
     SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill_rows, tb_cap, adaptive);
     const int warps = warps_per_block;
-    const int blocks = sms * blocks_per_sm;
+    int occ = 0;
+    if (warps == 4) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<4>, 4 * 32, 0);
+    else if (warps == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<8>, 8 * 32, 0);
+    else if (warps == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<2>, 2 * 32, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<1>, 32, 0);
+    // every block must be resident at once (persistent kernel): never more than the occupancy allows
+    const int per_sm = std::max(1, std::min(blocks_per_sm, occ));
+    const int blocks = sms * per_sm;
     const int64_t slots = (int64_t)blocks * warps;
     ensure(&d_slots_, &d_slots_cap_, (size_t)(slots * L.bytes));
     stats.slots = (int32_t)slots;

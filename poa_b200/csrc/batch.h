@@ -49,7 +49,7 @@ class BatchEngine {
     void sync_stats();
     BatchStats stats;
     int32_t warps_per_block = 4;
-    int32_t blocks_per_sm = 4;
+    int32_t blocks_per_sm = 8;  // upper bound; the occupancy calculator decides
 
   private:
     void ensure(void** ptr, size_t* cap, size_t bytes);

@@ -7,6 +7,8 @@
 #include <string>
 
 #include "../../include/poa_b200.h"
+#include <cuda_runtime.h>
+
 #include "batch.h"
 #include "gpu_engine.h"
 
@@ -305,6 +307,16 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
     const pb::BatchStats& s = ctx->batch->stats;
     o[0] = s.cells; o[1] = s.failed; o[2] = s.slots; o[3] = s.slot_bytes; o[4] = s.h2d_bytes; o[5] = s.d2h_bytes;
     return POA_OK;
+}
+
+void* poa_alloc_pinned(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void poa_free_pinned(void* ptr) {
+    if (ptr) cudaFreeHost(ptr);
 }
 
 int poa_stats(const poa_ctx* ctx, int64_t* o) {

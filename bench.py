@@ -194,16 +194,16 @@ def run_cpu_windows(binary, paths, cores):
 
 
 def cpu_sample(ws, seconds, cores, binary):
-    """Windows/s of the CPU binary on windows 0.. of ws, about `seconds` of work."""
+    """Windows/s of the CPU binary over windows 0, 1, ... of ws: chunks of
+    4 windows per core until about `seconds` of wall time have passed."""
+    outs = []
+    n = 0
     with tempfile.TemporaryDirectory() as d:
-        probe = write_windows(ws, range(min(cores, ws.n_windows)), d)
         t0 = time.perf_counter()
-        run_cpu_windows(binary, probe, cores)
-        per = (time.perf_counter() - t0) / max(len(probe), 1) * cores  # seconds per window per core
-        n = int(min(ws.n_windows, max(cores, seconds * cores / max(per, 1e-3))))
-        paths = write_windows(ws, range(n), d)
-        t0 = time.perf_counter()
-        outs = run_cpu_windows(binary, paths, cores)
+        while n < ws.n_windows and time.perf_counter() - t0 < seconds:
+            idx = range(n, min(ws.n_windows, n + 4 * cores))
+            outs.extend(run_cpu_windows(binary, write_windows(ws, idx, d), cores))
+            n = idx.stop
         dt = time.perf_counter() - t0
     return n / dt, n, dt, outs
 
@@ -286,6 +286,7 @@ def ours(args, world, rank, local, D):
         "cells_per_step": cells, "failed_windows": failed,
         "gpu_launches": args.steps, "e2e": e2e, "roofline": roofline, "clocks": clocks,
         "slots": st["slots"], "slot_bytes": st["slot_bytes"],
+        "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN

@@ -130,8 +130,10 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
                         const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows,
                         char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status);
 /* [0] band cells of the last run, [1] windows that failed, [2] concurrent
- * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes. */
-int poa_batch_stats(poa_ctx* ctx, int64_t* out6);
+ * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes,
+ * [6..11] summed per-window clock cycles of the view build, DP fill,
+ * backtrack, graph fusion, topological sort and consensus phases. */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out12);
 
 /* Page-locked host memory (cudaMallocHost) for callers that want the
  * batch copies to run at full PCIe/NVLink-C2C speed; NULL on failure. */

@@ -229,9 +229,11 @@ class Context:
         return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
 
     def batch_stats(self) -> dict:
-        o = (ctypes.c_int64 * 6)()
+        o = (ctypes.c_int64 * 12)()
         self._check(lib().poa_batch_stats(self._h, o))
-        return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5])
+        names = ("view", "fill", "backtrack", "fusion", "topsort", "consensus")
+        return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5],
+                    phase_cycles={names[k]: o[6 + k] for k in range(6)})
 
     def set_timing(self, on: bool = True):
         lib().poa_set_timing(self._h, 1 if on else 0)

@@ -87,7 +87,11 @@ struct BatchArgs {
     int32_t* cons_len;
     int32_t* status;
     int64_t* cells;
+    int64_t* phase;  // [n_windows * NPHASE] lane-0 clock cycles per phase
 };
+
+// per-window cycle counters (clock64 on lane 0): where a window's time goes
+enum { PH_VIEW = 0, PH_FILL, PH_BT, PH_FUSE, PH_SORT, PH_CONS, NPHASE = 8 };
 
 // Pointers of one slot's device graph.
 struct DevGraph {
@@ -307,6 +311,13 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
     const bool lens = A.f > 0;
     int status = ST_OK;
     int64_t cells = 0;
+    long long ph[NPHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long tc = clock64();
+    auto tick = [&](int k) {
+        long long t = clock64();
+        ph[k] += t - tc;
+        tc = t;
+    };
     for (int x = lane; x < L.NC; x += 32) { g.hlen[x] = 0; g.tlen[x] = 0; }
     if (lane == 0) {
         int nn = 0;
@@ -333,13 +344,16 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
                 g.hdr[0] = nn;
                 g.hdr[1] = ne;
+                tick(PH_FUSE);
                 if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
+                tick(PH_SORT);
                 g.hdr[2] = st;
             }
             __syncwarp();
             status = g.hdr[2];
             continue;
         }
+        tick(PH_FUSE);
         // DP rows of the whole graph and the shifted query
         WinView v;
         const int beg_i = build_view(g, s, L, v, lane);
@@ -368,13 +382,16 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         }
         __syncwarp();
         if (v.n > L.NC) { status = ST_CAPACITY; break; }
+        tick(PH_VIEW);
         dp_fill(grp, a);
         __syncwarp();
+        tick(PH_FILL);
         if (lane == 0) {
             int st = a.out[0];
             cells += a.out[3];
             int32_t nm = 0;
             if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
+            tick(PH_BT);
             if (st == ST_OK) {
                 // moves -> path -> fusion (src/align.cpp:1606-1620, 1672-1682; src/graph.cpp:170-235)
                 int nn = g.hdr[0], ne = g.hdr[1], anchored = -1;
@@ -407,7 +424,9 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
                 g.hdr[0] = nn;
                 g.hdr[1] = ne;
+                tick(PH_FUSE);
                 if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
+                tick(PH_SORT);
             }
             g.hdr[2] = st;
         }
@@ -420,9 +439,11 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             len = dg_consensus(g, g.hdr[0], A.cons + (int64_t)w * A.cons_stride, A.cons_stride);
             if (len < 0) status = ST_CAPACITY;
         }
+        tick(PH_CONS);
         A.cons_len[w] = len < 0 ? 0 : len;
         A.status[w] = status;
         A.cells[w] = cells;
+        for (int k = 0; k < NPHASE; k++) A.phase[(int64_t)w * NPHASE + k] = ph[k];
     }
     __syncwarp();
 }
@@ -523,6 +544,7 @@ void BatchEngine::upload(const BatchInput& in, const Params& p) {
     out_len_ = o; o = up256(o + 4 * (size_t)n_windows_);
     out_status_ = o; o = up256(o + 4 * (size_t)n_windows_);
     out_cells_ = o; o = up256(o + 8 * (size_t)n_windows_);
+    out_phase_ = o; o = up256(o + 8 * (size_t)NPHASE * n_windows_);
     out_bytes_ = o;
     ensure(&d_out_, &d_out_cap_, o);
     if (h_out_cap_ < o) {
@@ -589,6 +611,7 @@ void BatchEngine::run() {
     A.cons_len = (int32_t*)(o + out_len_);
     A.status = (int32_t*)(o + out_status_);
     A.cells = (int64_t*)(o + out_cells_);
+    A.phase = (int64_t*)(o + out_phase_);
     cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
     cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
     if (warps == 4) k_batch<4><<<blocks, 4 * 32, 0, s>>>(A);
@@ -611,11 +634,14 @@ void BatchEngine::sync_stats() {
     cuda_check(cudaStreamSynchronize(s), "D2H stats");
     const int32_t* st = (const int32_t*)(h + out_status_);
     const int64_t* cl = (const int64_t*)(h + out_cells_);
+    const int64_t* ph = (const int64_t*)(h + out_phase_);
     stats.cells = 0;
     stats.failed = 0;
+    for (int k = 0; k < 8; k++) stats.phase_cycles[k] = 0;
     for (int w = 0; w < n_windows_; w++) {
         stats.cells += cl[w];
         stats.failed += st[w] != ST_OK;
+        for (int k = 0; k < NPHASE; k++) stats.phase_cycles[k] += ph[(int64_t)w * NPHASE + k];
     }
 }
 

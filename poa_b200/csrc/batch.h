@@ -33,6 +33,9 @@ struct BatchStats {
     int64_t h2d_bytes = 0, d2h_bytes = 0;
     int32_t failed = 0;       // windows that ended with a non-OK status
     int32_t retried = 0;      // windows re-run with larger capacities
+    // summed lane-0 clock cycles per phase over all windows: view build, DP
+    // fill, backtrack, fusion, topological sort, consensus
+    int64_t phase_cycles[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 class BatchEngine {
@@ -66,7 +69,7 @@ class BatchEngine {
     void* d_slots_ = nullptr;   size_t d_slots_cap_ = 0;
     void* h_out_ = nullptr;     size_t h_out_cap_ = 0;   // pinned mirror of d_out_
     size_t off_seq_ = 0, off_roff_ = 0, off_rlen_ = 0, off_woff_ = 0, off_order_ = 0, off_ctr_ = 0;
-    size_t out_cons_ = 0, out_len_ = 0, out_status_ = 0, out_cells_ = 0, out_bytes_ = 0;
+    size_t out_cons_ = 0, out_len_ = 0, out_status_ = 0, out_cells_ = 0, out_phase_ = 0, out_bytes_ = 0;
     std::vector<int32_t> order_;
 };
 

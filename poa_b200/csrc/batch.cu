@@ -36,6 +36,7 @@ struct SlotLayout {
     int64_t e_from, e_to, e_w, e_nin, e_nout;
     int64_t rank_to_id, hlen, tlen, deg, stk, pre, score;
     int64_t v_in_ptr, v_in_row, v_in_w, v_in_base, v_out_ptr, v_out_row, v_base, v_ind, v_hq, v_hq_loc, v_tq;
+    int64_t v_pmeta;
     int64_t meta, state, qs, moves, rs, tb;
     int64_t bytes;
 };
@@ -60,6 +61,7 @@ SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, in
     L.v_in_ptr = take(n4 + 4); L.v_in_row = take(e4); L.v_in_w = take(e4); L.v_in_base = take(EC);
     L.v_out_ptr = take(n4 + 4); L.v_out_row = take(e4); L.v_base = take(NC); L.v_ind = take(n4);
     L.v_hq = take(n4); L.v_hq_loc = take(n4); L.v_tq = take(n4);
+    L.v_pmeta = take(8 * (size_t)EC);
     L.meta = take(sizeof(RowMeta) * (size_t)NC);
     L.state = take(adaptive ? 4 * (size_t)AB_NSTATE * NC : 64);
     L.qs = take((size_t)qs_bytes(QC) + 64);
@@ -82,6 +84,9 @@ struct BatchArgs {
     int32_t b, f, ab_band;
     char* slots;
     SlotLayout L;
+    int32_t smem_per_warp;   // bytes of dynamic shared memory per warp
+    int32_t sring_rows;      // shared-memory ring rows of the static-band fill (0 = all rows in global)
+    int32_t sring_blocks;    // blocks per ring row
     char* cons;
     int32_t cons_stride;
     int32_t* cons_len;
@@ -229,6 +234,384 @@ __device__ int dg_consensus(DevGraph& g, int nn, char* out, int cap) {
     return len;
 }
 
+// Topological sort with the whole warp: the out-lists are copied into
+// shared memory as CSR (16-bit ids), the LIFO Kahn loop of
+// src/graph.cpp:61-85 then runs on lane 0 over shared memory only, and
+// hlen/tlen (src/graph.cpp:86-123) are depths in the heaviest-in-edge and
+// heaviest-out-edge forests, computed by pointer jumping across the warp
+// (double-buffered in the slot's scratch arrays). Graphs too large for the
+// shared-memory budget use the sequential global-memory version.
+__device__ void dg_topsort_warp(DevGraph& g, int nn, int ne, bool with_lens, uint16_t* sm, int sm_bytes,
+                                int lane) {
+    const size_t need = 2 * ((size_t)nn + 1) + 2 * (size_t)ne + 4 * (size_t)nn + 16;
+    if (nn >= 65535 || ne >= 65535 || need > (size_t)sm_bytes) {
+        if (lane == 0) g.hdr[3] = dg_topsort(g, nn, with_lens);
+        __syncwarp();
+        return;
+    }
+    uint16_t* optr = sm;
+    uint16_t* adj = optr + nn + 1;
+    uint16_t* deg = adj + ne;
+    uint16_t* stk = deg + nn;
+    int carry = 0;
+    for (int c0 = 0; c0 < nn; c0 += 32) {
+        const int u = c0 + lane;
+        const int c = u < nn ? g.out_cnt[u] : 0;
+        int x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (u < nn) optr[u] = (uint16_t)(carry + x - c);
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) optr[nn] = (uint16_t)carry;
+    for (int u = lane; u < nn; u += 32) {
+        int k = 0;
+        const int base_k = (int)optr[u];
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) adj[base_k + k++] = (uint16_t)g.e_to[e];
+        deg[u] = (uint16_t)g.in_cnt[u];
+    }
+    __syncwarp();
+    // zero in-degree seeds in id order
+    int sp = 0;
+    for (int c0 = 0; c0 < nn; c0 += 32) {
+        const int u = c0 + lane;
+        const bool z = u < nn && deg[u] == 0;
+        const unsigned msk = __ballot_sync(0xffffffffu, z);
+        if (z) stk[sp + __popc(msk & ((1u << lane) - 1u))] = (uint16_t)u;
+        sp += __popc(msk);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int nr = 0;
+        while (sp) {
+            const int u = stk[--sp];
+            g.rank[u] = nr;
+            g.rank_to_id[nr++] = u;
+            const int k1 = optr[u + 1];
+            for (int k = optr[u]; k < k1; k++) {
+                const int v = adj[k];
+                const int dv = deg[v] - 1;
+                deg[v] = (uint16_t)dv;
+                if (dv == 0) stk[sp++] = (uint16_t)v;
+            }
+        }
+        g.hdr[3] = nr;
+    }
+    __syncwarp();
+    if (!with_lens) return;
+    for (int pass = 0; pass < 2; pass++) {
+        // pass 0: hlen over heaviest predecessors; pass 1: tlen over heaviest successors
+        int32_t *P = g.deg, *Q = g.stk, *D = g.pre, *E = g.score;
+        int32_t* arr = pass == 0 ? g.hlen : g.tlen;
+        for (int u = lane; u < nn; u += 32) {
+            int wmax = -1, best = -1;
+            if (pass == 0) {
+                for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e])
+                    if (g.e_w[e] > wmax) { wmax = g.e_w[e]; best = g.e_from[e]; }
+            } else {
+                for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
+                    if (g.e_w[e] > wmax) { wmax = g.e_w[e]; best = g.e_to[e]; }
+            }
+            P[u] = best;
+            D[u] = best >= 0 ? 1 : ((pass == 1 && u == 1) ? 1 : arr[g.rank[u]]);
+        }
+        __syncwarp();
+        for (int it = 0; it < 40; it++) {
+            bool moved = false;
+            for (int u = lane; u < nn; u += 32) {
+                const int p = P[u];
+                if (p >= 0) {
+                    E[u] = D[u] + D[p];
+                    Q[u] = P[p];
+                    moved = true;
+                } else {
+                    E[u] = D[u];
+                    Q[u] = -1;
+                }
+            }
+            __syncwarp();
+            int32_t* t = P; P = Q; Q = t;
+            t = D; D = E; E = t;
+            if (!__any_sync(0xffffffffu, moved)) break;
+        }
+        for (int u = lane; u < nn; u += 32) arr[g.rank[u]] = D[u];
+        __syncwarp();
+    }
+}
+
+// Static-band view (f > 0, no adaptive band): besides the predecessor lists,
+// every row's band, row-store location and record offset are a pure function
+// of hlen/tlen, so the warp computes them all here, in parallel, and attaches
+// to each in-edge the predecessor's (Bs, Be, location). The fill then needs
+// one coalesced load per predecessor and no per-row bookkeeping.
+// Row store location: ring slot -(r % R) - 1 in shared memory, or an offset
+// in the slot's spill area for rows with a successor R or more rows ahead.
+__device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinView& v, int m, int f, int wband,
+                                 int R, int RB, int lane, int& beg_out) {
+    const int beg_i = g.rank[0], end_i = g.rank[1];
+    const int n = end_i - beg_i + 1;
+    beg_out = beg_i;
+    int32_t* in_ptr = (int32_t*)(s + L.v_in_ptr);
+    int32_t* in_row = (int32_t*)(s + L.v_in_row);
+    int32_t* in_w = (int32_t*)(s + L.v_in_w);
+    uint8_t* in_base = (uint8_t*)(s + L.v_in_base);
+    int32_t* vind = (int32_t*)(s + L.v_ind);
+    int2* pmeta = (int2*)(s + L.v_pmeta);
+    RowMeta* meta = (RowMeta*)(s + L.meta);
+    const int h0 = g.hlen[beg_i], t0 = g.tlen[end_i];
+    const int64_t spill_cap = L.rs_cap;
+    // pass 1: per-row counts, band, widths
+    for (int r = lane; r < n; r += 32) {
+        const int u = g.rank_to_id[beg_i + r];
+        int ci = 0, maxs = r;
+        for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e]) ci += (g.rank[g.e_from[e]] - beg_i >= 0);
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) {
+            const int sr = g.rank[g.e_to[e]] - beg_i;
+            if (sr < n && sr > maxs) maxs = sr;
+        }
+        int Bs, Be;
+        band_static(f, g.hlen[beg_i + r] - h0, g.tlen[beg_i + r] - t0, m, wband, Bs, Be);
+        if (r == 0) Bs = 0;
+        const int bn = Be - Bs - 1;
+        const int d = r == 0 ? 0 : ci;
+        const int bpc = d >= 2 ? 4 : 1;
+        const bool spill = R == 0 || (maxs - r >= R) || bn > RB;
+        in_ptr[r + 1] = ci;
+        vind[r] = g.ind[u];
+        RowMeta rm;
+        rm.Bs = Bs;
+        rm.Be = Be;
+        rm.tb = bn > 0 ? (((int64_t)bn * BLK * bpc + 15) & ~(int64_t)15) : 0;   // widths, scanned below
+        rm.st = spill ? (bn > 0 ? (int64_t)bn * 16 : 0) : -1;
+        if (bn < 0 || d > MAX_MULTI_PRED) rm.Be = INT32_MIN;                  // flagged
+        meta[r] = rm;
+    }
+    __syncwarp();
+    // scans: in_ptr, record offsets, spill offsets
+    int ci_c = 0;
+    int64_t tb_c = 0, sp_c = 0;
+    bool bad = false;
+    if (lane == 0) in_ptr[0] = 0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+        const int r = c0 + lane;
+        RowMeta rm;
+        int ci = 0;
+        int64_t tbw = 0, spw = 0;
+        bool sp = false;
+        if (r < n) {
+            rm = meta[r];
+            ci = in_ptr[r + 1];
+            tbw = rm.tb;
+            sp = rm.st >= 0;
+            spw = sp ? rm.st : 0;
+            bad |= rm.Be == INT32_MIN;
+        }
+        int xi = ci;
+        long long xt = tbw, xs = spw;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int yi = __shfl_up_sync(0xffffffffu, xi, o);
+            const long long yt = __shfl_up_sync(0xffffffffu, xt, o);
+            const long long ys = __shfl_up_sync(0xffffffffu, xs, o);
+            if (lane >= o) { xi += yi; xt += yt; xs += ys; }
+        }
+        if (r < n) {
+            in_ptr[r + 1] = ci_c + xi;
+            rm.tb = tb_c + (xt - tbw);
+            rm.st = sp ? sp_c + (xs - spw) : -(int64_t)(r % (R > 0 ? R : 1)) - 1;
+            meta[r] = rm;
+        }
+        ci_c += __shfl_sync(0xffffffffu, xi, 31);
+        tb_c += __shfl_sync(0xffffffffu, xt, 31);
+        sp_c += __shfl_sync(0xffffffffu, xs, 31);
+    }
+    if (__any_sync(0xffffffffu, bad)) return ST_DEGENERATE;
+    if (tb_c > L.tb_cap || sp_c > spill_cap) return ST_OOM;
+    __syncwarp();
+    // pass 2: predecessor lists in in-list order
+    for (int r = lane; r < n; r += 32) {
+        const int u = g.rank_to_id[beg_i + r];
+        int k = in_ptr[r];
+        for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e]) {
+            const int p = g.rank[g.e_from[e]] - beg_i;
+            if (p < 0) continue;
+            in_row[k] = p;
+            in_w[k] = g.e_w[e];
+            in_base[k] = p == 0 ? 4 : g.base[g.e_from[e]];
+            k++;
+        }
+    }
+    __syncwarp();
+    // pass 3: predecessor metadata per in-edge
+    const int E = in_ptr[n];
+    for (int e = lane; e < E; e += 32) {
+        const RowMeta pm = meta[in_row[e]];
+        pmeta[e] = make_int2(pm.Bs | (pm.Be << 16), (int32_t)pm.st);
+    }
+    __syncwarp();
+    v.n = n;
+    v.in_ptr = in_ptr; v.in_row = in_row; v.in_w = in_w; v.in_base = in_base;
+    v.ind = vind;
+    return ST_OK;
+}
+
+// Static-band DP fill of one alignment by one warp (see build_view_static).
+// Same per-block arithmetic as dp_fill (plain.cuh); rows live in a
+// shared-memory ring of R rows or in the spill area.
+__device__ void dp_fill_warp_static(const DpArgs& a, const int2* __restrict__ pmeta, int32_t* ring, int RB,
+                                    int lane) {
+    const int n = a.v.n, m = a.qlen + 1;
+    const Scoring sc = a.sc;
+    int64_t cells = 0;
+    for (int i = 0; i < n; i++) {
+        const RowMeta rm = a.meta[i];
+        const int e0 = a.v.in_ptr[i];
+        const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
+        const int Bs = rm.Bs, bn = rm.Be - rm.Bs - 1;
+        int32_t* dst = rm.st < 0 ? ring + (int64_t)(-rm.st - 1) * RB * 16 : a.rs + rm.st;
+        cells += (int64_t)bn * BLK;
+        const int nch = (bn + 31) >> 5;
+        int32_t carryP = 0, carryM = NEG_INF, carryI = NEG_INF;
+        bool haveP = false;
+        for (int c = 0; c < nch; c++) {
+            const int b = c * 32 + lane;
+            const bool act = b < bn;
+            const int B = Bs + b;
+            int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
+            int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
+            PredMask cmk;
+            cmk.blk_in = cmk.prev_in = cmk.diag = false;
+            uint8_t qc8[BLK];
+#pragma unroll
+            for (int l = 0; l < BLK; l++) {
+                Mpre[l] = NEG_INF;
+                Dv[l] = NEG_INF;
+                cMb[l] = cDb[l] = NEG_INF;
+            }
+            if (act) {
+                load_qc8(a.qs, B, qc8);
+                if (i == 0) {
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) Mpre[l] = (b == 0 && l == 0) ? 0 : NEG_INF;
+                }
+                for (int e = e0; e < e0 + d; e++) {
+                    const int2 pm = pmeta[e];
+                    const int pBs = pm.x & 0xffff, pBe = pm.x >> 16;
+                    const int32_t* src = pm.y < 0 ? ring + (int64_t)(-pm.y - 1) * RB * 16 : a.rs + pm.y;
+                    const PredMask mk = pred_mask(B, pBs, pBe);
+                    int32_t Mb[BLK], Db[BLK];
+                    int32_t mprev = NEG_INF;
+                    if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                    if (mk.blk_in) {
+                        load_block16(src + (B - pBs) * 16, Mb, Db);
+                        pass1_pred(sc, mk, b == 0, a.v.in_base[e], Mb, Db, mprev, qc8, Mpre, Dv);
+                    }
+                    if (d == 1) {
+                        cmk = mk;
+                        cmprev = mprev;
+                        if (mk.blk_in) {
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
+                        }
+                    }
+                }
+            }
+            int32_t agg = INT_MIN;
+#pragma unroll
+            for (int l = 0; l < BLK; l++) {
+                H0[l] = mx(Mpre[l], Dv[l]);
+                if (act) agg = mx(agg, scan_key(H0[l], b * BLK + l, sc.e1));
+            }
+            const int32_t incl = warp_incl_max(agg);
+            int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) P = INT_MIN;
+            const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
+            if (haveP) P = mx(P, carryP);
+            if (act) {
+                if (i == 0) {
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
+                } else {
+                    finalize_block(sc, b * BLK, P, H0, M, I);
+                }
+            } else {
+#pragma unroll
+                for (int l = 0; l < BLK; l++) { M[l] = NEG_INF; I[l] = NEG_INF; }
+            }
+            const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
+            const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
+            const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
+            const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
+            const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
+            if (act) {
+                FlagAcc acc;
+                flag_acc_init(acc);
+                if (d == 1) {
+                    if (cmk.blk_in || cmk.prev_in)
+                        flags_pred(sc, cmk, a.v.in_base[e0], a.v.in_w[e0], 0, cMb, cDb, cmprev, qc8, M, Dv, acc);
+                } else {
+                    for (int e = e0; e < e0 + d; e++) {
+                        const int2 pm = pmeta[e];
+                        const int pBs = pm.x & 0xffff, pBe = pm.x >> 16;
+                        const int32_t* src = pm.y < 0 ? ring + (int64_t)(-pm.y - 1) * RB * 16 : a.rs + pm.y;
+                        const PredMask mk = pred_mask(B, pBs, pBe);
+                        if (!(mk.blk_in || mk.prev_in)) continue;
+                        int32_t Mb[BLK], Db[BLK];
+                        int32_t mprev = NEG_INF;
+                        if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                        if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
+                        else {
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                        }
+                        flags_pred(sc, mk, a.v.in_base[e], a.v.in_w[e], e - e0, Mb, Db, mprev, qc8, M, Dv, acc);
+                    }
+                }
+                const int ind = a.v.ind[i];
+                if (d >= 2) {
+                    uint32_t r[BLK];
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                        r[l] = encode_wide(own_flags(sc, b * BLK + l, M[l], Dv[l], I[l], Ml, Il), acc, l, ind);
+                    }
+                    uint4* tdst = reinterpret_cast<uint4*>(a.tb + rm.tb + (int64_t)b * BLK * 4);
+                    tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
+                    tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
+                } else {
+                    uint32_t lo = 0, hi = 0;
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                        const uint32_t v = encode_small(own_flags(sc, b * BLK + l, M[l], Dv[l], I[l], Ml, Il), acc, l, ind);
+                        if (l < 4) lo |= v << (8 * l);
+                        else hi |= v << (8 * (l - 4));
+                    }
+                    *reinterpret_cast<uint2*>(a.tb + rm.tb + (int64_t)b * BLK) = make_uint2(lo, hi);
+                }
+                store_block16(dst + (int64_t)b * 16, M, Dv);
+            }
+            carryP = haveP ? mx(carryP, chunk_total) : chunk_total;
+            haveP = true;
+            carryM = nextM;
+            carryI = nextI;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        const RowMeta last = a.meta[n - 1];
+        const int jm = m - last.Bs * BLK;
+        const int32_t* src = last.st < 0 ? ring + (int64_t)(-last.st - 1) * RB * 16 : a.rs + last.st;
+        a.out[1] = src[(jm / BLK) * 16 + jm % BLK];
+        a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+        a.out[0] = ST_OK;
+    }
+    __syncwarp();
+}
+
 // Build the DP rows of window [rank(source), rank(sink)] with the whole warp.
 __device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v, int lane) {
     const int beg_i = g.rank[0], end_i = g.rank[1];
@@ -304,11 +687,14 @@ __device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v,
     return beg_i;
 }
 
-__device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared* sr, int w, int lane) {
+template <bool STATIC>
+__device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared* sr, unsigned char* wsm, int w,
+                               int lane) {
     const SlotLayout& L = A.L;
     DevGraph g = slot_graph(s, L);
     const int r0 = A.win_off[w], r1 = A.win_off[w + 1];
     const bool lens = A.f > 0;
+    constexpr bool static_band = STATIC;  // f > 0 && !ab_band (checked on the host)
     int status = ST_OK;
     int64_t cells = 0;
     long long ph[NPHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -344,19 +730,27 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
                 g.hdr[0] = nn;
                 g.hdr[1] = ne;
-                tick(PH_FUSE);
-                if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
-                tick(PH_SORT);
                 g.hdr[2] = st;
             }
             __syncwarp();
             status = g.hdr[2];
+            tick(PH_FUSE);
+            if (status == ST_OK && r + 1 < r1)
+                dg_topsort_warp(g, g.hdr[0], g.hdr[1], lens, (uint16_t*)wsm, A.smem_per_warp, lane);
+            tick(PH_SORT);
             continue;
         }
         tick(PH_FUSE);
         // DP rows of the whole graph and the shifted query
         WinView v;
-        const int beg_i = build_view(g, s, L, v, lane);
+        int beg_i;
+        if constexpr (static_band) {
+            const int st = build_view_static(g, s, L, v, len + 1, A.f, A.b + (len + 1) / A.f, A.sring_rows,
+                                             A.sring_blocks, lane, beg_i);
+            if (st != ST_OK) { status = st; break; }
+        } else {
+            beg_i = build_view(g, s, L, v, lane);
+        }
         uint8_t* qs = (uint8_t*)(s + L.qs);
         const int64_t qsb = qs_bytes(len);
         for (int64_t x = lane; x < qsb; x += 32) qs[x] = (x >= 2 && x < len + 2) ? nt4_dev(rd[x - 2]) : 4;
@@ -383,7 +777,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         __syncwarp();
         if (v.n > L.NC) { status = ST_CAPACITY; break; }
         tick(PH_VIEW);
-        dp_fill(grp, a);
+        if constexpr (static_band) dp_fill_warp_static(a, (const int2*)(s + L.v_pmeta), (int32_t*)wsm, A.sring_blocks, lane);
+        else dp_fill(grp, a);
         __syncwarp();
         tick(PH_FILL);
         if (lane == 0) {
@@ -424,14 +819,15 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
                 g.hdr[0] = nn;
                 g.hdr[1] = ne;
-                tick(PH_FUSE);
-                if (st == ST_OK && r + 1 < r1) dg_topsort(g, nn, lens);
-                tick(PH_SORT);
             }
             g.hdr[2] = st;
         }
         __syncwarp();
         status = g.hdr[2];
+        tick(PH_FUSE);
+        if (status == ST_OK && r + 1 < r1)
+            dg_topsort_warp(g, g.hdr[0], g.hdr[1], lens, (uint16_t*)wsm, A.smem_per_warp, lane);
+        tick(PH_SORT);
     }
     if (lane == 0) {
         int len = -1;
@@ -448,19 +844,21 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
     __syncwarp();
 }
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_batch(BatchArgs A) {
+template <int WARPS, bool STATIC>
+__global__ void __launch_bounds__(WARPS * 32, 12 / WARPS) k_batch(BatchArgs A) {
     __shared__ DpArgs s_args[WARPS];
     __shared__ RowShared s_sr[WARPS];
+    extern __shared__ __align__(16) unsigned char dsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * WARPS + warp;
     char* s = A.slots + slot * A.L.bytes;
+    unsigned char* wsm = dsm + (size_t)warp * A.smem_per_warp;
     while (true) {
         int idx = 0;
         if (lane == 0) idx = atomicAdd(A.counter, 1);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= A.n_windows) break;
-        process_window(A, s, s_args[warp], &s_sr[warp], A.order[idx], lane);
+        process_window<STATIC>(A, s, s_args[warp], &s_sr[warp], wsm, A.order[idx], lane);
     }
 }
 
@@ -577,11 +975,21 @@ void BatchEngine::run() {
     const int64_t tb_cap = (int64_t)NC * ring_blocks * BLK * 2 + 4096;
     SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill_rows, tb_cap, adaptive);
     const int warps = warps_per_block;
+    const int smem_w = smem_per_warp;
+    const size_t dyn = (size_t)warps * smem_w;
+    // static band: shared-memory ring of up to 8 rows of ring_blocks blocks
+    int sring_blocks = ring_blocks;
+    int sring_rows = std::min(8, smem_w / std::max(1, sring_blocks * 64));
+    if (sring_rows < 2) sring_rows = 0;
     int occ = 0;
-    if (warps == 4) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<4>, 4 * 32, 0);
-    else if (warps == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<8>, 8 * 32, 0);
-    else if (warps == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<2>, 2 * 32, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batch<1>, 32, 0);
+    auto occ_of = [&](auto kern) {
+        cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn), "smem attr");
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, warps * 32, dyn), "occupancy");
+    };
+    const bool stat = p_.f > 0 && !p_.ab_band;
+    if (warps != 4) throw std::invalid_argument("batch kernel is built for 4 warps per block");
+    if (stat) occ_of(k_batch<4, true>);
+    else occ_of(k_batch<4, false>);
     // every block must be resident at once (persistent kernel): never more than the occupancy allows
     const int per_sm = std::max(1, std::min(blocks_per_sm, occ));
     const int blocks = sms * per_sm;
@@ -606,6 +1014,9 @@ void BatchEngine::run() {
     A.ab_band = p_.ab_band;
     A.slots = (char*)d_slots_;
     A.L = L;
+    A.smem_per_warp = smem_w;
+    A.sring_rows = sring_rows;
+    A.sring_blocks = sring_blocks;
     A.cons = o + out_cons_;
     A.cons_stride = cons_stride_;
     A.cons_len = (int32_t*)(o + out_len_);
@@ -614,10 +1025,8 @@ void BatchEngine::run() {
     A.phase = (int64_t*)(o + out_phase_);
     cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
     cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
-    if (warps == 4) k_batch<4><<<blocks, 4 * 32, 0, s>>>(A);
-    else if (warps == 8) k_batch<8><<<blocks, 8 * 32, 0, s>>>(A);
-    else if (warps == 2) k_batch<2><<<blocks, 2 * 32, 0, s>>>(A);
-    else k_batch<1><<<blocks, 32, 0, s>>>(A);
+    if (stat) k_batch<4, true><<<blocks, 4 * 32, dyn, s>>>(A);
+    else k_batch<4, false><<<blocks, 4 * 32, dyn, s>>>(A);
     cuda_check(cudaGetLastError(), "k_batch launch");
     cuda_check(cudaEventRecord((cudaEvent_t)ev1_, s), "event");
     cuda_check(cudaEventSynchronize((cudaEvent_t)ev1_), "k_batch");

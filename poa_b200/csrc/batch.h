@@ -53,6 +53,7 @@ class BatchEngine {
     BatchStats stats;
     int32_t warps_per_block = 4;
     int32_t blocks_per_sm = 8;  // upper bound; the occupancy calculator decides
+    int32_t smem_per_warp = 16384;  // shared-memory row ring / topsort workspace per warp
 
   private:
     void ensure(void** ptr, size_t* cap, size_t bytes);

@@ -287,6 +287,7 @@ def ours(args, world, rank, local, D):
         "gpu_launches": args.steps, "e2e": e2e, "roofline": roofline, "clocks": clocks,
         "slots": st["slots"], "slot_bytes": st["slot_bytes"],
         "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
+        "phase_mcycles_per_window": {k: v / 1e6 / ws.n_windows for k, v in st["phase_cycles"].items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN

@@ -135,6 +135,12 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * backtrack, graph fusion, topological sort and consensus phases. */
 int poa_batch_stats(poa_ctx* ctx, int64_t* out12);
 
+/* Launch shape of the batch kernel (the autotuner's knobs): key 0 = blocks
+ * per SM upper bound (the occupancy calculator still caps it), 1 = maximum
+ * number of blocks in total (0 = no cap), 2 = shared memory per warp in
+ * bytes (row ring + topsort workspace). Takes effect at the next run. */
+int poa_batch_config(poa_ctx* ctx, int32_t key, int64_t value);
+
 /* Page-locked host memory (cudaMallocHost) for callers that want the
  * batch copies to run at full PCIe/NVLink-C2C speed; NULL on failure. */
 void* poa_alloc_pinned(size_t bytes);

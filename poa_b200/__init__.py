@@ -116,6 +116,7 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, _i64p, _i32p]
     L.poa_batch_stats.argtypes = [ctypes.c_void_p, _i64p]
     L.poa_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.poa_batch_config.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
     L.poa_alloc_pinned.restype = ctypes.c_void_p
     L.poa_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
@@ -227,6 +228,12 @@ class Context:
         self._nwin = nwin
         raw = cons.raw
         return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
+
+    def batch_config(self, blocks_per_sm=None, max_blocks=None, smem_per_warp=None):
+        """Launch shape of the batch kernel (see poa_batch_config)."""
+        for key, val in ((0, blocks_per_sm), (1, max_blocks), (2, smem_per_warp)):
+            if val is not None:
+                self._check(lib().poa_batch_config(self._h, key, int(val)))
 
     def batch_stats(self) -> dict:
         o = (ctypes.c_int64 * 12)()

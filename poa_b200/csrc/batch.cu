@@ -992,7 +992,8 @@ void BatchEngine::run() {
     else occ_of(k_batch<4, false>);
     // every block must be resident at once (persistent kernel): never more than the occupancy allows
     const int per_sm = std::max(1, std::min(blocks_per_sm, occ));
-    const int blocks = sms * per_sm;
+    int blocks = sms * per_sm;
+    if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
     const int64_t slots = (int64_t)blocks * warps;
     ensure(&d_slots_, &d_slots_cap_, (size_t)(slots * L.bytes));
     stats.slots = (int32_t)slots;

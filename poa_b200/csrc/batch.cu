@@ -36,7 +36,7 @@ struct SlotLayout {
     int64_t e_from, e_to, e_w, e_nin, e_nout;
     int64_t rank_to_id, hlen, tlen, deg, stk, pre, score;
     int64_t v_in_ptr, v_in_row, v_in_w, v_in_base, v_out_ptr, v_out_row, v_base, v_ind, v_hq, v_hq_loc, v_tq;
-    int64_t v_pmeta;
+    int64_t v_pmeta, v_desc;
     int64_t meta, state, qs, moves, rs, tb;
     int64_t bytes;
 };
@@ -61,7 +61,8 @@ SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, in
     L.v_in_ptr = take(n4 + 4); L.v_in_row = take(e4); L.v_in_w = take(e4); L.v_in_base = take(EC);
     L.v_out_ptr = take(n4 + 4); L.v_out_row = take(e4); L.v_base = take(NC); L.v_ind = take(n4);
     L.v_hq = take(n4); L.v_hq_loc = take(n4); L.v_tq = take(n4);
-    L.v_pmeta = take(8 * (size_t)EC);
+    L.v_pmeta = take(16 * (size_t)EC);
+    L.v_desc = take(48 * (size_t)NC);
     L.meta = take(sizeof(RowMeta) * (size_t)NC);
     L.state = take(adaptive ? 4 * (size_t)AB_NSTATE * NC : 64);
     L.qs = take((size_t)qs_bytes(QC) + 64);
@@ -342,6 +343,16 @@ __device__ void dg_topsort_warp(DevGraph& g, int nn, int ne, bool with_lens, uin
     }
 }
 
+// Everything the static-band fill needs about one row, in one 48-byte record
+// (three 16-byte loads, issued one row ahead): the band, where the row's M/D
+// blocks and records go, its predecessor range, and the first predecessor's
+// band/location/base/weight so single-predecessor rows need nothing else.
+struct __align__(16) RowDesc {
+    int32_t bsbe, st, tb, e0;      // Bs | Be << 16, row store location, record offset, first in-edge
+    int32_t d, ind, w1ok, pad0;    // in-window predecessors, in-degree count, in_weight >= ind/10 (first pred)
+    int32_t pbsbe, pst, pbase, pw; // first predecessor: band, location, base (as the DP sees it), in_weight
+};
+
 // Static-band view (f > 0, no adaptive band): besides the predecessor lists,
 // every row's band, row-store location and record offset are a pure function
 // of hlen/tlen, so the warp computes them all here, in parallel, and attaches
@@ -359,7 +370,8 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
     int32_t* in_w = (int32_t*)(s + L.v_in_w);
     uint8_t* in_base = (uint8_t*)(s + L.v_in_base);
     int32_t* vind = (int32_t*)(s + L.v_ind);
-    int2* pmeta = (int2*)(s + L.v_pmeta);
+    int4* erec = (int4*)(s + L.v_pmeta);
+    RowDesc* desc = (RowDesc*)(s + L.v_desc);
     RowMeta* meta = (RowMeta*)(s + L.meta);
     const int h0 = g.hlen[beg_i], t0 = g.tlen[end_i];
     const int64_t spill_cap = L.rs_cap;
@@ -449,7 +461,31 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
     const int E = in_ptr[n];
     for (int e = lane; e < E; e += 32) {
         const RowMeta pm = meta[in_row[e]];
-        pmeta[e] = make_int2(pm.Bs | (pm.Be << 16), (int32_t)pm.st);
+        erec[e] = make_int4(pm.Bs | (pm.Be << 16), (int32_t)pm.st, in_w[e], in_base[e]);
+    }
+    __syncwarp();
+    // pass 4: row descriptors
+    for (int r = lane; r < n; r += 32) {
+        const RowMeta rm = meta[r];
+        const int e0 = in_ptr[r];
+        const int d = r == 0 ? 0 : in_ptr[r + 1] - e0;
+        RowDesc rd;
+        rd.bsbe = rm.Bs | (rm.Be << 16);
+        rd.st = (int32_t)rm.st;
+        rd.tb = (int32_t)rm.tb;
+        rd.e0 = e0;
+        rd.d = d;
+        rd.ind = vind[r];
+        rd.pad0 = 0;
+        if (d >= 1) {
+            const int4 er = erec[e0];
+            rd.pbsbe = er.x; rd.pst = er.y; rd.pw = er.z; rd.pbase = er.w;
+            rd.w1ok = er.z >= rd.ind / 10;
+        } else {
+            rd.pbsbe = rd.pst = rd.pw = rd.pbase = 0;
+            rd.w1ok = 0;
+        }
+        desc[r] = rd;
     }
     __syncwarp();
     v.n = n;
@@ -459,87 +495,101 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
 }
 
 // Static-band DP fill of one alignment by one warp (see build_view_static).
-// Same per-block arithmetic as dp_fill (plain.cuh); rows live in a
-// shared-memory ring of R rows or in the spill area.
-__device__ void dp_fill_warp_static(const DpArgs& a, const int2* __restrict__ pmeta, int32_t* ring, int RB,
-                                    int lane) {
+// Same recurrences and records as dp_fill (plain.cuh), specialised for the
+// batch: row descriptors prefetched one row ahead, the query in shared
+// memory, the previous rows' M/D in a shared-memory ring, the horizontal gap
+// recurrence in the form I[j] = o1 + (j-1)*e1 + max(K, max_{k<j} H0[k]-k*e1)
+// with K = NEG_INF + e1 - o1 (which also yields I[0] = NEG_INF), and the
+// one-byte records of single-predecessor rows built without the weight keys.
+__device__ __forceinline__ RowDesc load_desc(const RowDesc* p) {
+    const int4* q = reinterpret_cast<const int4*>(p);
+    const int4 a = q[0], b = q[1], c = q[2];
+    RowDesc r;
+    r.bsbe = a.x; r.st = a.y; r.tb = a.z; r.e0 = a.w;
+    r.d = b.x; r.ind = b.y; r.w1ok = b.z; r.pad0 = b.w;
+    r.pbsbe = c.x; r.pst = c.y; r.pbase = c.z; r.pw = c.w;
+    return r;
+}
+
+__device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__ desc, const int4* __restrict__ erec,
+                                    int32_t* ring, int RB, const uint8_t* qsm, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
     const Scoring sc = a.sc;
+    const int32_t K = add32(add32(NEG_INF, sc.e1), -sc.o1);
     int64_t cells = 0;
+    RowDesc cur = load_desc(desc);
     for (int i = 0; i < n; i++) {
-        const RowMeta rm = a.meta[i];
-        const int e0 = a.v.in_ptr[i];
-        const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
-        const int Bs = rm.Bs, bn = rm.Be - rm.Bs - 1;
-        int32_t* dst = rm.st < 0 ? ring + (int64_t)(-rm.st - 1) * RB * 16 : a.rs + rm.st;
+        RowDesc nxt;
+        if (i + 1 < n) nxt = load_desc(desc + i + 1);
+        const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
+        const int d = cur.d;
+        int32_t* dst = cur.st < 0 ? ring + (-cur.st - 1) * RB * 16 : a.rs + cur.st;
         cells += (int64_t)bn * BLK;
         const int nch = (bn + 31) >> 5;
-        int32_t carryP = 0, carryM = NEG_INF, carryI = NEG_INF;
-        bool haveP = false;
+        int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
         for (int c = 0; c < nch; c++) {
             const int b = c * 32 + lane;
             const bool act = b < bn;
             const int B = Bs + b;
+            const int j0 = b * BLK;
             int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
             int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
-            PredMask cmk;
-            cmk.blk_in = cmk.prev_in = cmk.diag = false;
+            bool c_blk = false, c_prev = false;
             uint8_t qc8[BLK];
 #pragma unroll
-            for (int l = 0; l < BLK; l++) {
-                Mpre[l] = NEG_INF;
-                Dv[l] = NEG_INF;
-                cMb[l] = cDb[l] = NEG_INF;
-            }
+            for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
             if (act) {
-                load_qc8(a.qs, B, qc8);
-                if (i == 0) {
+                const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
 #pragma unroll
-                    for (int l = 0; l < BLK; l++) Mpre[l] = (b == 0 && l == 0) ? 0 : NEG_INF;
-                }
-                for (int e = e0; e < e0 + d; e++) {
-                    const int2 pm = pmeta[e];
-                    const int pBs = pm.x & 0xffff, pBe = pm.x >> 16;
-                    const int32_t* src = pm.y < 0 ? ring + (int64_t)(-pm.y - 1) * RB * 16 : a.rs + pm.y;
+                for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qw.x >> (8 * l)); qc8[4 + l] = (uint8_t)(qw.y >> (8 * l)); }
+                if (i == 0 && b == 0) Mpre[0] = 0;
+                for (int k = 0; k < d; k++) {
+                    int pbsbe, pst, pbase;
+                    if (k == 0) { pbsbe = cur.pbsbe; pst = cur.pst; pbase = cur.pbase; }
+                    else { const int4 er = erec[cur.e0 + k]; pbsbe = er.x; pst = er.y; pbase = er.w; }
+                    const int pBs = pbsbe & 0xffff, pBe = pbsbe >> 16;
+                    const int32_t* src = pst < 0 ? ring + (-pst - 1) * RB * 16 : a.rs + pst;
                     const PredMask mk = pred_mask(B, pBs, pBe);
                     int32_t Mb[BLK], Db[BLK];
                     int32_t mprev = NEG_INF;
                     if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
                     if (mk.blk_in) {
                         load_block16(src + (B - pBs) * 16, Mb, Db);
-                        pass1_pred(sc, mk, b == 0, a.v.in_base[e], Mb, Db, mprev, qc8, Mpre, Dv);
-                    }
-                    if (d == 1) {
-                        cmk = mk;
-                        cmprev = mprev;
-                        if (mk.blk_in) {
+                        pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+                        if (d == 1) {
 #pragma unroll
                             for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
                         }
                     }
+                    if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
                 }
             }
+            // prefix max of the scan keys across the warp
+            int32_t key[BLK];
             int32_t agg = INT_MIN;
 #pragma unroll
             for (int l = 0; l < BLK; l++) {
                 H0[l] = mx(Mpre[l], Dv[l]);
-                if (act) agg = mx(agg, scan_key(H0[l], b * BLK + l, sc.e1));
+                key[l] = add32(H0[l], -(j0 + l) * sc.e1);
+                agg = mx(agg, key[l]);
             }
+            if (!act) agg = INT_MIN;
             const int32_t incl = warp_incl_max(agg);
             int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
             if (lane == 0) P = INT_MIN;
+            P = mx(P, carryP);
             const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
-            if (haveP) P = mx(P, carryP);
-            if (act) {
-                if (i == 0) {
+            if (i == 0) {
 #pragma unroll
-                    for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
-                } else {
-                    finalize_block(sc, b * BLK, P, H0, M, I);
-                }
+                for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
             } else {
+                int32_t run = P;
 #pragma unroll
-                for (int l = 0; l < BLK; l++) { M[l] = NEG_INF; I[l] = NEG_INF; }
+                for (int l = 0; l < BLK; l++) {
+                    I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
+                    M[l] = mx(H0[l], I[l]);
+                    run = mx(run, key[l]);
+                }
             }
             const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
             const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
@@ -547,16 +597,33 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const int2* __restrict__ pm
             const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
             const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
             if (act) {
-                FlagAcc acc;
-                flag_acc_init(acc);
-                if (d == 1) {
-                    if (cmk.blk_in || cmk.prev_in)
-                        flags_pred(sc, cmk, a.v.in_base[e0], a.v.in_w[e0], 0, cMb, cDb, cmprev, qc8, M, Dv, acc);
+                if (d <= 1) {
+                    uint32_t lo = 0, hi = 0;
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                        uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
+                        if (d == 1) {
+                            const bool inr = l == 0 ? c_prev : c_blk;
+                            const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
+                            const bool bm = cur.pbase == qc8[l];
+                            const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                            if (eqM) r |= R_M4;
+                            if (eqM && bm && cur.w1ok) r |= R_M1;
+                            if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
+                            else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
+                        }
+                        if (l < 4) lo |= r << (8 * l);
+                        else hi |= r << (8 * (l - 4));
+                    }
+                    *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
                 } else {
-                    for (int e = e0; e < e0 + d; e++) {
-                        const int2 pm = pmeta[e];
-                        const int pBs = pm.x & 0xffff, pBe = pm.x >> 16;
-                        const int32_t* src = pm.y < 0 ? ring + (int64_t)(-pm.y - 1) * RB * 16 : a.rs + pm.y;
+                    FlagAcc acc;
+                    flag_acc_init(acc);
+                    for (int k = 0; k < d; k++) {
+                        const int4 er = erec[cur.e0 + k];
+                        const int pBs = er.x & 0xffff, pBe = er.x >> 16;
+                        const int32_t* src = er.y < 0 ? ring + (-er.y - 1) * RB * 16 : a.rs + er.y;
                         const PredMask mk = pred_mask(B, pBs, pBe);
                         if (!(mk.blk_in || mk.prev_in)) continue;
                         int32_t Mb[BLK], Db[BLK];
@@ -567,38 +634,25 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const int2* __restrict__ pm
 #pragma unroll
                             for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
                         }
-                        flags_pred(sc, mk, a.v.in_base[e], a.v.in_w[e], e - e0, Mb, Db, mprev, qc8, M, Dv, acc);
+                        flags_pred(sc, mk, er.w, er.z, k, Mb, Db, mprev, qc8, M, Dv, acc);
                     }
-                }
-                const int ind = a.v.ind[i];
-                if (d >= 2) {
                     uint32_t r[BLK];
 #pragma unroll
                     for (int l = 0; l < BLK; l++) {
                         const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                        r[l] = encode_wide(own_flags(sc, b * BLK + l, M[l], Dv[l], I[l], Ml, Il), acc, l, ind);
+                        r[l] = encode_wide(own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il), acc, l, cur.ind);
                     }
-                    uint4* tdst = reinterpret_cast<uint4*>(a.tb + rm.tb + (int64_t)b * BLK * 4);
+                    uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
                     tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
                     tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
-                } else {
-                    uint32_t lo = 0, hi = 0;
-#pragma unroll
-                    for (int l = 0; l < BLK; l++) {
-                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                        const uint32_t v = encode_small(own_flags(sc, b * BLK + l, M[l], Dv[l], I[l], Ml, Il), acc, l, ind);
-                        if (l < 4) lo |= v << (8 * l);
-                        else hi |= v << (8 * (l - 4));
-                    }
-                    *reinterpret_cast<uint2*>(a.tb + rm.tb + (int64_t)b * BLK) = make_uint2(lo, hi);
                 }
-                store_block16(dst + (int64_t)b * 16, M, Dv);
+                store_block16(dst + b * 16, M, Dv);
             }
-            carryP = haveP ? mx(carryP, chunk_total) : chunk_total;
-            haveP = true;
+            carryP = mx(carryP, chunk_total);
             carryM = nextM;
             carryI = nextI;
         }
+        cur = nxt;
         __syncwarp();
     }
     if (lane == 0) {
@@ -777,8 +831,17 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         __syncwarp();
         if (v.n > L.NC) { status = ST_CAPACITY; break; }
         tick(PH_VIEW);
-        if constexpr (static_band) dp_fill_warp_static(a, (const int2*)(s + L.v_pmeta), (int32_t*)wsm, A.sring_blocks, lane);
-        else dp_fill(grp, a);
+        if constexpr (static_band) {
+            // the query goes after the row ring in this warp's shared memory
+            uint8_t* qsm = wsm + (size_t)A.sring_rows * A.sring_blocks * 64;
+            for (int64_t x = lane * 16; x < qsb; x += 32 * 16)
+                *reinterpret_cast<uint4*>(qsm + x) = *reinterpret_cast<const uint4*>(qs + x);
+            __syncwarp();
+            dp_fill_warp_static(a, (const RowDesc*)(s + L.v_desc), (const int4*)(s + L.v_pmeta), (int32_t*)wsm,
+                                A.sring_blocks, qsm, lane);
+        } else {
+            dp_fill(grp, a);
+        }
         __syncwarp();
         tick(PH_FILL);
         if (lane == 0) {
@@ -979,8 +1042,11 @@ void BatchEngine::run() {
     const size_t dyn = (size_t)warps * smem_w;
     // static band: shared-memory ring of up to 8 rows of ring_blocks blocks
     int sring_blocks = ring_blocks;
-    int sring_rows = std::min(8, smem_w / std::max(1, sring_blocks * 64));
+    const int qsm_bytes = (int)((qs_bytes(QC) + 15) / 16 * 16);
+    int sring_rows = std::min(8, (smem_w - qsm_bytes) / std::max(1, sring_blocks * 64));
     if (sring_rows < 2) sring_rows = 0;
+    if (p_.f > 0 && !p_.ab_band && qsm_bytes > smem_w)
+        throw std::invalid_argument("reads too long for the batch kernel's shared memory; raise smem_per_warp");
     int occ = 0;
     auto occ_of = [&](auto kern) {
         cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn), "smem attr");

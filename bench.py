@@ -221,6 +221,8 @@ def ours(args, world, rank, local, D):
     except Exception:
         pass
     ctx = poa_b200.Context(poa_b200.Params(), device=local)
+    if args.max_blocks:
+        ctx.batch_config(max_blocks=args.max_blocks)
 
     # ---- device-resident leg
     ctx.batch_upload(ws)
@@ -343,6 +345,8 @@ def main():
     ap.add_argument("--ref-windows-per-step", type=int, default=40)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--max-blocks", type=int, default=0,
+                    help="cap the persistent grid (small profiling captures); 0 = one full wave")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

@@ -175,6 +175,11 @@ def profile_traffic_per_cell():
     return d.get("dram_bytes_per_cell")
 
 
+def int_peak_ops(sm_mhz):
+    """Nominal int32 ALU peak: 148 SMs x 128 lanes x SM clock (no measured figure exists)."""
+    return 148 * 128 * (sm_mhz or 1965.0) * 1e6
+
+
 # --------------------------------------------------------------------- CPU leg
 def write_windows(ws, idx, d):
     from poa_b200 import synth

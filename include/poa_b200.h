@@ -135,6 +135,58 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * backtrack, graph fusion, topological sort and consensus phases. */
 int poa_batch_stats(poa_ctx* ctx, int64_t* out12);
 
+/* One poa() alignment on inputs already in device memory, without
+ * allocating anything (no counterpart in the reference).
+ *
+ * For callers that cannot allocate at the time they align: code inside a
+ * framework that owns the device memory pool, or a latency-bound service
+ * that forbids cudaMalloc on its request path (cudaMalloc synchronises the
+ * device and can fail under memory pressure). All arrays below are device
+ * pointers the caller owns; the DP's working memory is a fixed array of
+ * POA_NOALLOC_SCRATCH_BYTES inside the library, present on every GPU that
+ * loads the library until the process exits.
+ *
+ * Limit: the window must fit that array at its worst case (every row at the
+ * full band width): roughly n_rows * (qlen/8 + 2) * 96 bytes plus
+ * n_rows * 48 bytes must stay under POA_NOALLOC_SCRATCH_BYTES (64 MiB), e.g.
+ * 1,500 rows with a 700 bp query, or 400 rows with a 10 kb query. Larger
+ * windows are rejected with POA_OOM before anything is launched.
+ *
+ * w: the window's rows (ranks beg..end), laid out like the rows poa_align
+ * builds: CSR predecessor lists in in-list order (predecessor row, its
+ * in_weight, its base with 'N' for row 0), node base and in-degree count per
+ * row, hq = hlen[rank]-hlen[beg], hq_loc = hlen[row]-hlen[beg],
+ * tq = tlen[rank]-tlen[end], CSR successor rows in out-list order.
+ * q_dev: encoded query (codes 0..4). moves_dev (capacity moves_cap >=
+ * n_rows + qlen + 1) receives the backtrack moves in backtrack order, each
+ * (pred_row << 5 | kind << 3 | base) with kind 0 match, 1 mismatch,
+ * 2 insertion; result_dev[4] receives status, score, number of moves and
+ * band cells. The call is asynchronous on `stream` (a cudaStream_t, NULL =
+ * default stream); the return value reports argument and launch errors only.
+ *
+ * The first call on each device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call reuses the same array: calls whose
+ * kernels may overlap on the GPU (several streams or host threads) race on
+ * it and must be serialised by the caller. */
+#define POA_NOALLOC_SCRATCH_BYTES (64u << 20)
+typedef struct {
+    int32_t n_rows;
+    const int32_t* in_ptr;    /* [n_rows + 1] */
+    const int32_t* in_row;
+    const int32_t* in_weight;
+    const uint8_t* in_base;
+    const uint8_t* base;      /* [n_rows] */
+    const int32_t* ind;
+    const int32_t* hq;
+    const int32_t* hq_loc;
+    const int32_t* tq;
+    const int32_t* out_ptr;   /* [n_rows + 1] */
+    const int32_t* out_row;
+} poa_dev_window;
+int poa_align_noalloc(const poa_dev_window* w, const uint8_t* q_dev, int32_t qlen, const poa_params* p,
+                      int32_t ab_band, int32_t* moves_dev, int32_t moves_cap, int32_t* result_dev, void* stream);
+
 /* Launch shape of the batch kernel (the autotuner's knobs): key 0 = blocks
  * per SM upper bound (the occupancy calculator still caps it), 1 = maximum
  * number of blocks in total (0 = no cap), 2 = shared memory per warp in

@@ -661,3 +661,28 @@ char *po_run(const po_params *p, int nseq, const char *const *seqs, const int *l
     po_graph_free(g);
     return out;
 }
+
+/* ------------------------------------------------------------------ export */
+void po_graph_sizes(const po_graph *g, int *n_nodes, int *n_in, int *n_out, int *n_ranks, int *n_lens) {
+    int ni = 0, no = 0;
+    for (int i = 0; i < g->n; i++) { ni += g->node[i].in.n; no += g->node[i].out.n; }
+    *n_nodes = g->n; *n_in = ni; *n_out = no; *n_ranks = g->rank.n; *n_lens = g->hlen.n;
+}
+
+void po_graph_export(const po_graph *g, uint8_t *base, int *rank, int *par, int *ind, int *aligned,
+                     int *in_ptr, int *in_id, int *in_w, int *out_ptr, int *out_id, int *rank_to_id,
+                     int *hlen, int *tlen) {
+    int ki = 0, ko = 0;
+    in_ptr[0] = out_ptr[0] = 0;
+    for (int i = 0; i < g->n; i++) {
+        const po_node *v = &g->node[i];
+        base[i] = v->base; rank[i] = v->rank; par[i] = v->par_id; ind[i] = v->ind;
+        for (int k = 0; k < 5; k++) aligned[5 * i + k] = v->aligned[k];
+        for (int k = 0; k < v->in.n; k++) { in_id[ki] = v->in.a[k]; in_w[ki] = v->in_w.a[k]; ki++; }
+        for (int k = 0; k < v->out.n; k++) out_id[ko++] = v->out.a[k];
+        in_ptr[i + 1] = ki; out_ptr[i + 1] = ko;
+    }
+    for (int r = 0; r < g->rank.n; r++) rank_to_id[r] = g->rank.a[r];
+    for (int r = 0; r < g->hlen.n; r++) hlen[r] = g->hlen.a[r];
+    for (int r = 0; r < g->tlen.n; r++) tlen[r] = g->tlen.a[r];
+}

@@ -74,6 +74,14 @@ char *po_msa(const po_graph *g, int nseq, int *ncol);
 char *po_run(const po_params *p, int nseq, const char *const *seqs, const int *lens,
              const char *const *names, int mode, int *scores, int *status);
 
+/* Flatten the graph for tests: sizes first (nodes, in-edges, out-edges,
+ * ranks, hlen entries), then the arrays (caller-allocated; aligned has
+ * 5 entries per node; in/out lists in list order as CSR). */
+void po_graph_sizes(const po_graph *g, int *n_nodes, int *n_in, int *n_out, int *n_ranks, int *n_lens);
+void po_graph_export(const po_graph *g, uint8_t *base, int *rank, int *par, int *ind, int *aligned,
+                     int *in_ptr, int *in_id, int *in_w, int *out_ptr, int *out_id, int *rank_to_id,
+                     int *hlen, int *tlen);
+
 /* Per-graph introspection used by tests (arrays valid until the next mutation). */
 const int *po_graph_rank_to_id(const po_graph *g, int *n);
 int po_graph_node_base(const po_graph *g, int id);

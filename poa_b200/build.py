@@ -74,7 +74,7 @@ def build(verbose: bool = False) -> str:
     if os.path.exists(main) and (not os.path.exists(CLI) or os.path.getmtime(main) > os.path.getmtime(CLI)
                                  or os.path.getmtime(LIB) > os.path.getmtime(CLI)):
         _run(["g++", "-O2", "-std=c++17", main, "-o", CLI, "-L" + PKG, "-lpoa_b200",
-              "-Wl,-rpath,$ORIGIN"])
+              "-Wl,-rpath,$ORIGIN", "-lz"])
     if verbose:
         print("built", LIB)
     return LIB

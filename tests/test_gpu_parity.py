@@ -64,3 +64,18 @@ def test_seeded_vs_oracle(name, gen, opts, oracle_bin, tmp_path):
     with poa_b200.Context(poa_b200.Params.from_cli(opts)) as ctx:
         got, _ = ctx.run(seqs, hdr)
     assert got == want
+
+
+CLI = os.path.join(os.path.dirname(HERE), "poa_b200", "minipoa_b200")
+CLI_CASES = ["cons_small", "msa_small", "noisy_adaptive", "cons_scoring", "edge_mixed_msa", "window_00"]
+
+
+@pytest.mark.parametrize("name", CLI_CASES)
+def test_cli_drop_in(name):
+    """minipoa_b200 prints exactly what minipoa prints, given the same options."""
+    case = [c for c in CASES if c["case"] == name][0]
+    fa = os.path.join(GOLD, name + ".fa")
+    res = subprocess.run([CLI, fa] + case["opts"], capture_output=True, timeout=120)
+    assert res.returncode == 0, res.stderr
+    with open(os.path.join(GOLD, name + ".out"), "rb") as fh:
+        assert res.stdout == fh.read()

@@ -51,7 +51,7 @@ typedef struct {
     int32_t band_b, band_f;                     /* -b -f: 100 40 */
     int32_t ab_band;                            /* -B: 0 */
     int32_t seeding;                            /* -S: 0 */
-    int32_t k, mm_w, poa_w;                     /* -k -w -W: 19 10 10000 */
+    int32_t k, mm_w, poa_w;                     /* -k -w -W: 19 10 0 (-W is read only when given) */
     int32_t thread;                             /* -t: 1 */
     int32_t result;                             /* -r: 0 consensus, 1 row-column MSA */
     int32_t progressive;                        /* -p: 0 */

@@ -25,7 +25,7 @@ int main(int argc, char **argv) {
     para->match = 2; para->mismatch = -4; para->gap_open1 = -4; para->gap_ext1 = -2;
     para->b = 100; para->f = 40; para->ab_band = false; para->k = 19; para->mm_w = 10;
     para->bw = 1000; para->progressive_poa = false; para->enable_seeding = false;
-    para->thread = 1; para->result = 0; para->verbose = 0; para->poa_w = 10000;
+    para->thread = 1; para->result = 0; para->verbose = 0; para->poa_w = 0;  // -W read only when given (src/main.cpp:49-51)
     std::string in, dump;
     for (int a = 1; a < argc; a++) {
         std::string o = argv[a];

@@ -54,7 +54,7 @@ class Params:
     seeding: bool = False   # -S
     k: int = 19             # -k
     mm_w: int = 10          # -w
-    poa_w: int = 10000      # -W
+    poa_w: int = 0          # -W (minipoa reads it only when given; 0 = unset)
     thread: int = 1         # -t
     result: int = 0         # -r (0 consensus, 1 MSA)
     progressive: bool = False  # -p

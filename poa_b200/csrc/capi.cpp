@@ -104,7 +104,7 @@ void poa_params_init(poa_params* p) {
     std::memset(p, 0, sizeof(*p));
     p->match = 2; p->mismatch = -4; p->gap_open = -4; p->gap_ext = -2;
     p->band_b = 100; p->band_f = 40;
-    p->k = 19; p->mm_w = 10; p->poa_w = 10000;
+    p->k = 19; p->mm_w = 10; p->poa_w = 0;
     p->thread = 1;
 }
 

@@ -50,6 +50,7 @@ enum Status : int32_t {
     ST_INDEGREE = 5,      // more in-window predecessors than the 4-byte record can index
     ST_DEGENERATE = 6,    // a band with Be-Bs < 1: the reference writes outside its row there
     ST_CAPACITY = 7,      // a batched window outgrew its device graph capacity
+    ST_UNSUPPORTED = 9,   // an option outside the path (-p)
 };
 
 // record layout -------------------------------------------------------------

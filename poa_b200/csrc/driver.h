@@ -17,7 +17,7 @@ struct Params {
     int32_t ab_band = 0;          // -B
     int32_t enable_seeding = 0;   // -S
     int32_t k = 19, mm_w = 10;    // minimizer k-mer / window, src/main.cpp:27-28
-    int32_t poa_w = 10000;        // -W, src/main.cpp:26
+    int32_t poa_w = 0;            // -W: read only when given (src/main.cpp:49-51), so 0 by default
     int32_t bw = 1000;            // src/main.cpp:65
     int32_t thread = 1;           // -t
     int32_t result = 0;           // -r: 0 consensus, 1 row-column MSA

@@ -84,7 +84,7 @@ void usage() {
                  "  -S, --seeding          minimizer seeding and anchoring\n"
                  "  -k, --k_mer INT        k-mer length [19]\n"
                  "  -w, --mm_w INT         minimizer window [10]\n"
-                 "  -W, --poa_w INT        minimum distance between anchors [10000]\n"
+                 "  -W, --poa_w INT        minimum distance between anchors [unset]\n"
                  "  -t, --thread INT       threads [1]\n"
                  "  -r, --result INT       0 consensus, 1 row-column MSA [0]\n"
                  "  -V, --verbose INT      verbose level [0]\n"

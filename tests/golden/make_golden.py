@@ -3,7 +3,8 @@
 Run from the repository root after ``make -C oracle ref`` (which compiles the
 reference's own sources into ``oracle/_ref/``):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # small cases
+    python tests/golden/make_golden.py --fullsize   # md5 of full-size runs
 
 For every case it writes ``<case>.fa`` (seeded synthetic input),
 ``<case>.out`` (the reference CLI's stdout, byte for byte) and, where the case
@@ -74,9 +75,41 @@ def cases():
     return out
 
 
+# Full-size configurations: inputs are regenerated from their seeds by the
+# tests; only the md5 of the reference's stdout is stored.
+FULLSIZE = [
+    ("config1_consensus_10x16569", "single_graph_consensus", dict(seed=1), []),
+    ("config2_msa_100x16500", "single_graph_msa", dict(seed=2), ["-S", "-r", "1"]),
+    ("config3_noisy_30x10k_adaptive", "noisy_long_reads", dict(seed=3), ["-B"]),
+    ("config3_noisy_30x10k_static", "noisy_long_reads", dict(seed=3), []),
+]
+
+
+def fullsize():
+    import hashlib
+    import time
+    out = []
+    for name, gen, kw, opts in FULLSIZE:
+        reads = getattr(synth, gen)(**kw)
+        fa = os.path.join("/tmp", name + ".fa")
+        synth.write_fasta(fa, reads)
+        t0 = time.time()
+        res = subprocess.run([REF_BIN, fa] + opts, capture_output=True, check=True)
+        dt = time.time() - t0
+        out.append({"case": name, "generator": gen, "kwargs": kw, "opts": opts,
+                    "md5": hashlib.md5(res.stdout).hexdigest(), "bytes": len(res.stdout),
+                    "reference_seconds": round(dt, 2)})
+        os.unlink(fa)
+    with open(os.path.join(HERE, "fullsize.json"), "w") as fh:
+        json.dump(out, fh, indent=1)
+
+
 def main():
     if not (os.path.exists(REF_BIN) and os.path.exists(HARNESS)):
         sys.exit("build the reference first: make -C oracle ref")
+    if "--fullsize" in sys.argv:
+        fullsize()
+        return
     manifest = []
     for name, reads, opts, dump in cases():
         fa = os.path.join(HERE, name + ".fa")

@@ -204,12 +204,12 @@ struct ModelEngine : DpEngine {
 extern "C" {
 
 // Run the whole driver with the model engine. params: match, mismatch,
-// gap_open, gap_ext, b, f, ab_band, result. Returns status; *text is malloc'd.
+// gap_open, gap_ext, b, f, ab_band, result, seeding. Returns status; *text is malloc'd.
 int model_run(int nseq, const char* const* seqs, const int* lens, const int* params, char** text,
-              int* scores) {
+              int* scores, int scores_cap) {
     Params p;
     p.match = params[0]; p.mismatch = params[1]; p.gap_open1 = params[2]; p.gap_ext1 = params[3];
-    p.b = params[4]; p.f = params[5]; p.ab_band = params[6]; p.result = params[7];
+    p.b = params[4]; p.f = params[5]; p.ab_band = params[6]; p.result = params[7]; p.enable_seeding = params[8];
     normalize_params(p);
     std::vector<std::string> s(nseq), headers;
     for (int i = 0; i < nseq; i++) s[i].assign(seqs[i], lens[i]);
@@ -221,7 +221,7 @@ int model_run(int nseq, const char* const* seqs, const int* lens, const int* par
     memcpy(*text, out.data(), out.size());
     (*text)[out.size()] = 0;
     if (scores)
-        for (size_t i = 0; i < sc.size(); i++) scores[i] = sc[i];
+        for (size_t i = 0; i < sc.size() && (int)i < scores_cap; i++) scores[i] = sc[i];
     return st;
 }
 

@@ -21,7 +21,7 @@ GOLD = os.path.join(HERE, "golden")
 LIB = os.path.join(HERE, "model", "build", "libpoa_model.so")
 
 with open(os.path.join(GOLD, "manifest.json")) as fh:
-    CASES = [c for c in json.load(fh) if "-S" not in c["opts"]]
+    CASES = json.load(fh)
 
 
 @pytest.fixture(scope="module")
@@ -36,21 +36,21 @@ def model():
     lib.model_run.restype = ctypes.c_int
     lib.model_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int),
                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p),
-                              ctypes.POINTER(ctypes.c_int)]
+                              ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.model_free.argtypes = [ctypes.c_void_p]
     return lib
 
 
 def opts_to_params(opts):
-    p = dict(M=2, X=-4, O=-4, E=-2, b=100, f=40, B=0, r=0)
+    p = dict(M=2, X=-4, O=-4, E=-2, b=100, f=40, B=0, r=0, S=0)
     it = iter(opts)
     for o in it:
         k = o.lstrip("-")
-        if k == "B":
-            p["B"] = 1
+        if k in ("B", "S"):
+            p[k] = 1
         else:
             p[k] = int(next(it))
-    return [p["M"], p["X"], p["O"], p["E"], p["b"], p["f"], p["B"], p["r"]]
+    return [p["M"], p["X"], p["O"], p["E"], p["b"], p["f"], p["B"], p["r"], p["S"]]
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
@@ -59,10 +59,10 @@ def test_model_matches_reference(case, model):
     n = len(seqs)
     arr = (ctypes.c_char_p * n)(*seqs)
     lens = (ctypes.c_int * n)(*[len(s) for s in seqs])
-    par = (ctypes.c_int * 8)(*opts_to_params(case["opts"]))
+    par = (ctypes.c_int * 9)(*opts_to_params(case["opts"]))
     out = ctypes.c_void_p()
     scores = (ctypes.c_int * (n + 1))()
-    st = model.model_run(n, arr, lens, par, ctypes.byref(out), scores)
+    st = model.model_run(n, arr, lens, par, ctypes.byref(out), scores, n + 1)
     text = ctypes.string_at(out.value)
     model.model_free(out)
     assert st == 0

@@ -34,10 +34,10 @@ struct SlotLayout {
     // byte offsets inside a slot
     int64_t hdr, base, par, aligned, ind, rank, in_head, in_tail, out_head, out_tail, in_cnt, out_cnt;
     int64_t e_from, e_to, e_w, e_nin, e_nout;
-    int64_t rank_to_id, hlen, tlen, deg, stk, pre, score;
+    int64_t rank_to_id, hlen, tlen, deg, stk, pre, score, hin, hout, stamp;
     int64_t v_in_ptr, v_in_row, v_in_w, v_in_base, v_out_ptr, v_out_row, v_base, v_ind, v_hq, v_hq_loc, v_tq;
     int64_t v_pmeta, v_desc;
-    int64_t meta, state, qs, moves, rs, tb;
+    int64_t meta, state, qs, moves, path, rs, tb;
     int64_t bytes;
 };
 
@@ -58,6 +58,7 @@ SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, in
     L.e_from = take(e4); L.e_to = take(e4); L.e_w = take(e4); L.e_nin = take(e4); L.e_nout = take(e4);
     L.rank_to_id = take(n4); L.hlen = take(n4); L.tlen = take(n4); L.deg = take(n4); L.stk = take(n4);
     L.pre = take(n4); L.score = take(n4);
+    L.hin = take(n4); L.hout = take(n4); L.stamp = take(n4);
     L.v_in_ptr = take(n4 + 4); L.v_in_row = take(e4); L.v_in_w = take(e4); L.v_in_base = take(EC);
     L.v_out_ptr = take(n4 + 4); L.v_out_row = take(e4); L.v_base = take(NC); L.v_ind = take(n4);
     L.v_hq = take(n4); L.v_hq_loc = take(n4); L.v_tq = take(n4);
@@ -67,6 +68,7 @@ SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, in
     L.state = take(adaptive ? 4 * (size_t)AB_NSTATE * NC : 64);
     L.qs = take((size_t)qs_bytes(QC) + 64);
     L.moves = take(4 * ((size_t)NC + QC + 16));
+    L.path = take(4 * ((size_t)NC + QC + 16));
     L.rs = take(4 * (size_t)L.rs_cap);
     L.tb = take((size_t)tb_cap);
     L.bytes = (int64_t)up256(o);
@@ -106,6 +108,7 @@ struct DevGraph {
     int32_t *par, *aligned, *ind, *rank, *in_head, *in_tail, *out_head, *out_tail, *in_cnt, *out_cnt;
     int32_t *e_from, *e_to, *e_w, *e_nin, *e_nout;
     int32_t *rank_to_id, *hlen, *tlen, *deg, *stk, *pre, *score;
+    int32_t *hin, *hout, *stamp;  // heaviest in/out edge (first max in list order); fusion stamps
     int32_t NC, EC;
 };
 
@@ -123,6 +126,7 @@ __device__ DevGraph slot_graph(char* s, const SlotLayout& L) {
     g.rank_to_id = (int32_t*)(s + L.rank_to_id); g.hlen = (int32_t*)(s + L.hlen); g.tlen = (int32_t*)(s + L.tlen);
     g.deg = (int32_t*)(s + L.deg); g.stk = (int32_t*)(s + L.stk); g.pre = (int32_t*)(s + L.pre);
     g.score = (int32_t*)(s + L.score);
+    g.hin = (int32_t*)(s + L.hin); g.hout = (int32_t*)(s + L.hout); g.stamp = (int32_t*)(s + L.stamp);
     g.NC = L.NC; g.EC = L.EC;
     return g;
 }
@@ -150,7 +154,21 @@ __device__ int dg_add_node(DevGraph& g, int& nn, uint8_t base) {
     g.ind[id] = 0;
     g.in_head[id] = g.in_tail[id] = g.out_head[id] = g.out_tail[id] = -1;
     g.in_cnt[id] = g.out_cnt[id] = 0;
+    g.hin[id] = g.hout[id] = -1;
+    g.stamp[id] = 0;
     return id;
+}
+
+// Keep hin[v] / hout[u] = the heaviest in/out edge, first in list order on
+// ties, after edge e (u -> v) gained weight or was appended. List order is
+// edge-id order (edges are only ever appended), and only e changed, so the new
+// heaviest is the old one or e.
+__device__ __forceinline__ void dg_heavy(DevGraph& g, int e, int u, int v) {
+    const int w = g.e_w[e];
+    int b = g.hin[v];
+    if (b < 0 || w > g.e_w[b] || (w == g.e_w[b] && e < b)) g.hin[v] = e;
+    b = g.hout[u];
+    if (b < 0 || w > g.e_w[b] || (w == g.e_w[b] && e < b)) g.hout[u] = e;
 }
 
 // graph::add_adj (src/graph.cpp:13-20, include/node.h:23-61); false when full
@@ -158,7 +176,11 @@ __device__ bool dg_add_adj(DevGraph& g, int& ne, int u, int v) {
     if (u == v) return true;
     g.ind[v]++;
     for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
-        if (g.e_to[e] == v) { g.e_w[e]++; return true; }
+        if (g.e_to[e] == v) {
+            g.e_w[e]++;
+            dg_heavy(g, e, u, v);
+            return true;
+        }
     if (ne >= g.EC) return false;
     const int e = ne++;
     g.e_from[e] = u; g.e_to[e] = v; g.e_w[e] = 1; g.e_nin[e] = -1; g.e_nout[e] = -1;
@@ -166,6 +188,7 @@ __device__ bool dg_add_adj(DevGraph& g, int& ne, int u, int v) {
     g.out_tail[u] = e; g.out_cnt[u]++;
     if (g.in_tail[v] >= 0) g.e_nin[g.in_tail[v]] = e; else g.in_head[v] = e;
     g.in_tail[v] = e; g.in_cnt[v]++;
+    dg_heavy(g, e, u, v);
     return true;
 }
 
@@ -233,6 +256,204 @@ __device__ int dg_consensus(DevGraph& g, int nn, char* out, int cap) {
     int k = len;
     for (int id = g.pre[1]; id != 0; id = g.pre[id]) out[--k] = nt[g.base[id]];
     return len;
+}
+
+// Sequential fusion of one backtrack path (lane 0): the reference's order of
+// node creation and edge insertion, one element at a time.
+__device__ int dg_fuse_seq(DevGraph& g, const int32_t* moves, int nm, int beg_i) {
+    int st = ST_OK;
+    int nn = g.hdr[0], ne = g.hdr[1], anchored = -1;
+    for (int t = nm - 1; t >= 0 && st == ST_OK; t--) {
+        const int32_t mv = moves[t];
+        const int kind = mv_kind(mv), qc = mv_qc(mv);
+        int cur;
+        if (kind == MV_INSERT) {
+            cur = dg_add_node(g, nn, (uint8_t)qc);
+        } else {
+            const int pre = g.rank_to_id[beg_i + mv_row(mv)];
+            if (kind == MV_MATCH) {
+                cur = pre;
+            } else {
+                const int par = g.par[pre];
+                cur = g.aligned[par * 5 + qc];
+                if (cur == -1) {
+                    cur = dg_add_node(g, nn, (uint8_t)qc);
+                    if (cur >= 0) {
+                        g.aligned[par * 5 + qc] = cur;
+                        g.par[cur] = par;
+                    }
+                }
+            }
+        }
+        if (cur < 0) { st = ST_CAPACITY; break; }
+        if (anchored != -1 && !dg_add_adj(g, ne, anchored, cur)) st = ST_CAPACITY;
+        anchored = cur;
+    }
+    if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
+    g.hdr[0] = nn;
+    g.hdr[1] = ne;
+    return st;
+}
+
+// Fusion of one backtrack path with the whole warp (src/graph.cpp:170-235,
+// path elements as emitted by src/align.cpp:1606-1620, 1672-1682).
+// Path element q (backtrack move nm-1-q) becomes a node id: the predecessor
+// row's node for a match, its parent's aligned sibling for a mismatch (new
+// when absent), a new node for an insertion. New nodes get ids in path order
+// (prefix sums). The path then adds edges (q -> q+1) and (last -> sink); in a
+// path every node occurs once, so every in-list, out-list, in-degree and
+// heaviest-edge slot is touched by one edge at most and the edges are applied
+// in parallel. A path that would create the same aligned node twice or visit
+// a node twice is detected (CAS claims, fusion stamps) and fused sequentially
+// instead. Returns ST_OK, ST_CAPACITY, or -1 for "use the sequential path".
+__device__ int dg_fuse_warp(DevGraph& g, const int32_t* moves, int nm, int beg_i, int32_t* path, int fid,
+                            int lane) {
+    const int nn0 = g.hdr[0], ne0 = g.hdr[1];
+    const unsigned lt = (1u << lane) - 1u;
+    bool conflict = false, full = false;
+    int new_total = 0;
+    for (int c0 = 0; c0 < nm; c0 += 32) {
+        const int q = c0 + lane;
+        bool is_new = false;
+        int cur = -1, par = -1, qc = 0, kind = MV_INSERT;
+        if (q < nm) {
+            const int32_t mv = moves[nm - 1 - q];
+            kind = mv_kind(mv);
+            qc = mv_qc(mv);
+            if (kind == MV_INSERT) {
+                is_new = true;
+            } else {
+                const int pre = g.rank_to_id[beg_i + mv_row(mv)];
+                if (kind == MV_MATCH) {
+                    cur = pre;
+                } else {
+                    par = g.par[pre];
+                    cur = g.aligned[par * 5 + qc];
+                    is_new = cur == -1;
+                }
+            }
+        }
+        const unsigned msk = __ballot_sync(0xffffffffu, is_new);
+        if (is_new) {
+            cur = nn0 + new_total + __popc(msk & lt);
+            if (cur >= g.NC) {
+                full = true;
+            } else {
+                g.base[cur] = (uint8_t)qc;
+                g.par[cur] = par >= 0 ? par : cur;
+#pragma unroll
+                for (int k = 0; k < 5; k++) g.aligned[cur * 5 + k] = -1;
+                g.aligned[cur * 5 + qc] = cur;
+                g.ind[cur] = 0;
+                g.in_head[cur] = g.in_tail[cur] = g.out_head[cur] = g.out_tail[cur] = -1;
+                g.in_cnt[cur] = g.out_cnt[cur] = 0;
+                g.hin[cur] = g.hout[cur] = -1;
+                if (par >= 0 && atomicCAS(&g.aligned[par * 5 + qc], -1, cur) != -1) conflict = true;
+            }
+        }
+        if (q < nm && cur >= 0 && cur < g.NC && atomicExch(&g.stamp[cur], fid) == fid) conflict = true;
+        if (q < nm) path[q] = cur;
+        new_total += __popc(msk);
+    }
+    const bool any_full = __any_sync(0xffffffffu, full);
+    const bool any_conflict = __any_sync(0xffffffffu, conflict);
+    if (any_full || any_conflict) {
+        // undo this path's aligned claims; the node slots past nn0 are simply not kept
+        __syncwarp();
+        for (int q = lane; q < nm; q += 32) {
+            const int cur = path[q];
+            if (cur >= nn0 && cur < g.NC && g.par[cur] != cur) {
+                const int par = g.par[cur];
+                atomicCAS(&g.aligned[par * 5 + g.base[cur]], cur, -1);
+            }
+        }
+        __syncwarp();
+        return any_full ? ST_CAPACITY : -1;
+    }
+    __syncwarp();
+    // edges: pair t joins path[t] -> path[t+1] (the last one -> sink)
+    int new_edges = 0;
+    bool efull = false;
+    for (int c0 = 0; c0 < nm; c0 += 32) {
+        const int t = c0 + lane;
+        int u = -1, v = -1, found = -1;
+        bool need = false;
+        if (t < nm) {
+            u = path[t];
+            v = t + 1 < nm ? path[t + 1] : 1;
+            if (u != v) {
+                for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
+                    if (g.e_to[e] == v) { found = e; break; }
+                need = found < 0;
+            }
+        }
+        const unsigned msk = __ballot_sync(0xffffffffu, need);
+        if (t < nm && u != v) {
+            g.ind[v]++;
+            if (found >= 0) {
+                g.e_w[found]++;
+                dg_heavy(g, found, u, v);
+            } else {
+                const int e = ne0 + new_edges + __popc(msk & lt);
+                if (e >= g.EC) {
+                    efull = true;
+                } else {
+                    g.e_from[e] = u; g.e_to[e] = v; g.e_w[e] = 1; g.e_nin[e] = -1; g.e_nout[e] = -1;
+                    if (g.out_tail[u] >= 0) g.e_nout[g.out_tail[u]] = e; else g.out_head[u] = e;
+                    g.out_tail[u] = e; g.out_cnt[u]++;
+                    if (g.in_tail[v] >= 0) g.e_nin[g.in_tail[v]] = e; else g.in_head[v] = e;
+                    g.in_tail[v] = e; g.in_cnt[v]++;
+                    dg_heavy(g, e, u, v);
+                }
+            }
+        }
+        new_edges += __popc(msk);
+        __syncwarp();
+    }
+    if (__any_sync(0xffffffffu, efull)) return ST_CAPACITY;
+    if (lane == 0) {
+        g.hdr[0] = nn0 + new_total;
+        g.hdr[1] = ne0 + new_edges;
+    }
+    __syncwarp();
+    return ST_OK;
+}
+
+// Depth of every node in the forest where each node's parent is the far end
+// of its heaviest in-edge (pass 0, hlen: src/graph.cpp:86-101) or heaviest
+// out-edge (pass 1, tlen: src/graph.cpp:103-121). Roots keep the value the
+// array already holds at their rank (the reference resizes the vector and
+// never writes there), except the sink, whose tlen is 1. Written back by rank.
+template <typename T>
+__device__ void depth_jump(DevGraph& g, int nn, int pass, int32_t* arr, T* P, T* Q, T* D, T* E, int lane) {
+    const T none = (T)-1;
+    for (int u = lane; u < nn; u += 32) {
+        const int e = pass == 0 ? g.hin[u] : g.hout[u];
+        const int par = e < 0 ? -1 : (pass == 0 ? g.e_from[e] : g.e_to[e]);
+        P[u] = par < 0 ? none : (T)par;
+        D[u] = par >= 0 ? (T)1 : (T)((pass == 1 && u == 1) ? 1 : arr[g.rank[u]]);
+    }
+    __syncwarp();
+    for (int it = 0; it < 40; it++) {
+        bool moved = false;
+        for (int u = lane; u < nn; u += 32) {
+            const T p = P[u];
+            if (p != none) {
+                E[u] = (T)(D[u] + D[p]);
+                Q[u] = P[p];
+                moved = true;
+            } else {
+                E[u] = D[u];
+                Q[u] = none;
+            }
+        }
+        __syncwarp();
+        T* t = P; P = Q; Q = t;
+        t = D; D = E; E = t;
+        if (!__any_sync(0xffffffffu, moved)) break;
+    }
+    for (int u = lane; u < nn; u += 32) arr[g.rank[u]] = (int32_t)D[u];
+    __syncwarp();
 }
 
 // Topological sort with the whole warp: the out-lists are copied into
@@ -303,43 +524,14 @@ __device__ void dg_topsort_warp(DevGraph& g, int nn, int ne, bool with_lens, uin
     }
     __syncwarp();
     if (!with_lens) return;
+    // hlen / tlen: depths in the forests of heaviest in-edges (hin) and
+    // heaviest out-edges (hout), by pointer jumping; 16-bit arrays in shared
+    // memory when they fit, the slot's int32 scratch otherwise
+    const bool sm_ok = 8 * (size_t)nn + 16 <= (size_t)sm_bytes;
     for (int pass = 0; pass < 2; pass++) {
-        // pass 0: hlen over heaviest predecessors; pass 1: tlen over heaviest successors
-        int32_t *P = g.deg, *Q = g.stk, *D = g.pre, *E = g.score;
         int32_t* arr = pass == 0 ? g.hlen : g.tlen;
-        for (int u = lane; u < nn; u += 32) {
-            int wmax = -1, best = -1;
-            if (pass == 0) {
-                for (int e = g.in_head[u]; e >= 0; e = g.e_nin[e])
-                    if (g.e_w[e] > wmax) { wmax = g.e_w[e]; best = g.e_from[e]; }
-            } else {
-                for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e])
-                    if (g.e_w[e] > wmax) { wmax = g.e_w[e]; best = g.e_to[e]; }
-            }
-            P[u] = best;
-            D[u] = best >= 0 ? 1 : ((pass == 1 && u == 1) ? 1 : arr[g.rank[u]]);
-        }
-        __syncwarp();
-        for (int it = 0; it < 40; it++) {
-            bool moved = false;
-            for (int u = lane; u < nn; u += 32) {
-                const int p = P[u];
-                if (p >= 0) {
-                    E[u] = D[u] + D[p];
-                    Q[u] = P[p];
-                    moved = true;
-                } else {
-                    E[u] = D[u];
-                    Q[u] = -1;
-                }
-            }
-            __syncwarp();
-            int32_t* t = P; P = Q; Q = t;
-            t = D; D = E; E = t;
-            if (!__any_sync(0xffffffffu, moved)) break;
-        }
-        for (int u = lane; u < nn; u += 32) arr[g.rank[u]] = D[u];
-        __syncwarp();
+        if (sm_ok) depth_jump<uint16_t>(g, nn, pass, arr, sm, sm + nn, sm + 2 * nn, sm + 3 * nn, lane);
+        else depth_jump<int32_t>(g, nn, pass, arr, g.deg, g.stk, g.pre, g.score, lane);
     }
 }
 
@@ -349,7 +541,7 @@ __device__ void dg_topsort_warp(DevGraph& g, int nn, int ne, bool with_lens, uin
 // band/location/base/weight so single-predecessor rows need nothing else.
 struct __align__(16) RowDesc {
     int32_t bsbe, st, tb, e0;      // Bs | Be << 16, row store location, record offset, first in-edge
-    int32_t d, ind, w1ok, pad0;    // in-window predecessors, in-degree count, in_weight >= ind/10 (first pred)
+    int32_t d, ind, w1ok, prow0;   // in-window predecessors, in-degree count, in_weight >= ind/10, first pred row
     int32_t pbsbe, pst, pbase, pw; // first predecessor: band, location, base (as the DP sees it), in_weight
 };
 
@@ -476,7 +668,7 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
         rd.e0 = e0;
         rd.d = d;
         rd.ind = vind[r];
-        rd.pad0 = 0;
+        rd.prow0 = d >= 1 ? in_row[e0] : 0;
         if (d >= 1) {
             const int4 er = erec[e0];
             rd.pbsbe = er.x; rd.pst = er.y; rd.pw = er.z; rd.pbase = er.w;
@@ -506,7 +698,7 @@ __device__ __forceinline__ RowDesc load_desc(const RowDesc* p) {
     const int4 a = q[0], b = q[1], c = q[2];
     RowDesc r;
     r.bsbe = a.x; r.st = a.y; r.tb = a.z; r.e0 = a.w;
-    r.d = b.x; r.ind = b.y; r.w1ok = b.z; r.pad0 = b.w;
+    r.d = b.x; r.ind = b.y; r.w1ok = b.z; r.prow0 = b.w;
     r.pbsbe = c.x; r.pst = c.y; r.pbase = c.z; r.pw = c.w;
     return r;
 }
@@ -664,6 +856,85 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         a.out[0] = ST_OK;
     }
     __syncwarp();
+}
+
+// Backtrack over the records (src/align.cpp:1572-1736, same decisions as
+// backtrack_records) with the whole warp. The path mostly steps
+// (i, j) -> (i-1, j-1), so lane k preloads the descriptor of row i-k and its
+// record at column acj-k; the walk consumes lane t's values through shuffles
+// while the path stays on that diagonal and preloads again from wherever it
+// leaves it. All lanes run the walk (uniform control flow); lane 0 stores
+// the moves.
+__device__ int bt_warp_static(const RowDesc* __restrict__ desc, const int32_t* __restrict__ in_row,
+                              const uint8_t* __restrict__ in_base, const uint8_t* __restrict__ tb,
+                              const uint8_t* __restrict__ qs, int n, int m, int32_t* moves, int moves_cap,
+                              int32_t& nm_out, int lane) {
+    int i = n - 1, acj = m, op = ALL_OP, nm = 0;
+    int status = ST_OK;
+    while ((i > 0 || acj > 0) && status == ST_OK) {
+        const int i0 = i, a0 = acj;
+        // preload: lane k -> (i0 - k, a0 - k)
+        const int ri = i0 - lane, cj = a0 - lane;
+        int bsbe = 0, tbo = 0, d = 0, e0 = 0, prow0 = 0, pbase = 0;
+        uint32_t rec = 0;
+        int qc = 4;
+        if (ri >= 0) {
+            const RowDesc rd = load_desc(desc + ri);
+            bsbe = rd.bsbe; tbo = rd.tb; d = rd.d; e0 = rd.e0; prow0 = rd.prow0; pbase = rd.pbase;
+            const int Bs = bsbe & 0xffff, Be = bsbe >> 16;
+            const int j = cj - Bs * BLK;
+            if (j >= 0 && j < (Be - Bs - 1) * BLK)
+                rec = d >= 2 ? *reinterpret_cast<const uint32_t*>(tb + tbo + j * 4) : (uint32_t)tb[tbo + j];
+            if (cj > 0) qc = qs[cj];
+        }
+        for (int t = 0; t < 32; t++) {
+            const int Bs_t = __shfl_sync(0xffffffffu, bsbe, t) & 0xffff;
+            const int Be_t = __shfl_sync(0xffffffffu, bsbe, t) >> 16;
+            const int d_t = __shfl_sync(0xffffffffu, d, t);
+            const int e0_t = __shfl_sync(0xffffffffu, e0, t);
+            const int prow_t = __shfl_sync(0xffffffffu, prow0, t);
+            const int pbase_t = __shfl_sync(0xffffffffu, pbase, t);
+            const uint32_t rec_t = __shfl_sync(0xffffffffu, rec, t);
+            const int qc_t = __shfl_sync(0xffffffffu, qc, t);
+            if (acj > (Be_t - 1) * BLK || acj < Bs_t * BLK) { status = ST_BAND_ESCAPE; break; }
+            const int j = acj - Bs_t * BLK;
+            if (j >= (Be_t - Bs_t - 1) * BLK) { status = ST_BT_FAIL; break; }
+            if (nm + 1 > moves_cap) { status = ST_OOM; break; }
+            const Rec r = d_t >= 2 ? decode_wide(rec_t) : decode_small((uint8_t)rec_t);
+            int ni = i, na = acj;
+            bool moved = false;
+            if ((op & M_OP) && acj > 0 && r.m1 >= 0) {
+                const int p = d_t >= 2 ? in_row[e0_t + r.m1] : prow_t;
+                const int pb = d_t >= 2 ? in_base[e0_t + r.m1] : pbase_t;
+                if (lane == 0) moves[nm] = mv_pack(pb == qc_t ? MV_MATCH : MV_MISMATCH, p, qc_t);
+                nm++;
+                op = ALL_OP; ni = p; na = acj - 1; moved = true;
+            } else if ((op & D_OP) && (op == D_OP || r.eqMD) && r.dpos >= 0) {
+                ni = d_t >= 2 ? in_row[e0_t + r.dpos] : prow_t;
+                op = r.dext ? D_OP : (M_OP | I_OP);
+                moved = true;
+            } else if ((op & I_OP) && acj > 0 && j >= 1 && (op == I_OP || r.eqMI) && (r.iopen || r.iext)) {
+                if (lane == 0) moves[nm] = mv_pack(MV_INSERT, 0, qc_t);
+                nm++;
+                op = r.iopen ? (M_OP | D_OP) : I_OP;
+                na = acj - 1; moved = true;
+            } else if ((op & M_OP) && acj > 0 && r.m4 >= 0) {
+                const int p = d_t >= 2 ? in_row[e0_t + r.m4] : prow_t;
+                const int pb = d_t >= 2 ? in_base[e0_t + r.m4] : pbase_t;
+                if (lane == 0) moves[nm] = mv_pack(pb == qc_t ? MV_MATCH : MV_MISMATCH, p, qc_t);
+                nm++;
+                op = ALL_OP; ni = p; na = acj - 1; moved = true;
+            }
+            if (!moved) { status = ST_BT_FAIL; break; }
+            i = ni;
+            acj = na;
+            if (!(i > 0 || acj > 0)) break;
+            if (t + 1 >= 32 || i != i0 - (t + 1) || acj != a0 - (t + 1)) break;
+        }
+    }
+    nm_out = nm;
+    __syncwarp();
+    return status;
 }
 
 // Build the DP rows of window [rank(source), rank(sink)] with the whole warp.
@@ -844,46 +1115,42 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         }
         __syncwarp();
         tick(PH_FILL);
-        if (lane == 0) {
+        if constexpr (static_band) {
+            int st = a.out[0];
+            int32_t nm = 0;
+            if (st == ST_OK)
+                st = bt_warp_static((const RowDesc*)(s + L.v_desc), a.v.in_row, a.v.in_base, a.tb, qs, v.n, len + 1,
+                                    a.moves, a.moves_cap, nm, lane);
+            if (lane == 0) {
+                cells += a.out[3];
+                g.hdr[2] = st;
+                g.hdr[9] = nm;
+                g.hdr[8] = g.hdr[8] + 1;  // fusion stamp, increasing over the slot's lifetime
+            }
+        } else if (lane == 0) {
             int st = a.out[0];
             cells += a.out[3];
             int32_t nm = 0;
             if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
-            tick(PH_BT);
-            if (st == ST_OK) {
-                // moves -> path -> fusion (src/align.cpp:1606-1620, 1672-1682; src/graph.cpp:170-235)
-                int nn = g.hdr[0], ne = g.hdr[1], anchored = -1;
-                for (int t = nm - 1; t >= 0 && st == ST_OK; t--) {
-                    const int32_t mv = a.moves[t];
-                    const int kind = mv_kind(mv), qc = mv_qc(mv);
-                    int cur;
-                    if (kind == MV_INSERT) {
-                        cur = dg_add_node(g, nn, (uint8_t)qc);
-                    } else {
-                        const int pre = g.rank_to_id[beg_i + mv_row(mv)];
-                        if (kind == MV_MATCH) {
-                            cur = pre;
-                        } else {
-                            const int par = g.par[pre];
-                            cur = g.aligned[par * 5 + qc];
-                            if (cur == -1) {
-                                cur = dg_add_node(g, nn, (uint8_t)qc);
-                                if (cur >= 0) {
-                                    g.aligned[par * 5 + qc] = cur;
-                                    g.par[cur] = par;
-                                }
-                            }
-                        }
-                    }
-                    if (cur < 0) { st = ST_CAPACITY; break; }
-                    if (anchored != -1 && !dg_add_adj(g, ne, anchored, cur)) st = ST_CAPACITY;
-                    anchored = cur;
-                }
-                if (st == ST_OK && !dg_add_adj(g, ne, anchored, 1)) st = ST_CAPACITY;
-                g.hdr[0] = nn;
-                g.hdr[1] = ne;
-            }
             g.hdr[2] = st;
+            g.hdr[9] = nm;
+            g.hdr[8] = g.hdr[8] + 1;
+        }
+        __syncwarp();
+        tick(PH_BT);
+        {
+            int st = g.hdr[2];
+            const int nm = g.hdr[9];
+            if (st == ST_OK) {
+                st = dg_fuse_warp(g, a.moves, nm, beg_i, (int32_t*)(s + L.path), g.hdr[8], lane);
+                if (st == -1) {
+                    // sequential fusion (a path that repeats a node or an aligned sibling)
+                    st = ST_OK;
+                    if (lane == 0) st = dg_fuse_seq(g, a.moves, nm, beg_i);
+                    __syncwarp();
+                }
+            }
+            if (lane == 0) g.hdr[2] = st;
         }
         __syncwarp();
         status = g.hdr[2];
@@ -1061,7 +1328,12 @@ void BatchEngine::run() {
     int blocks = sms * per_sm;
     if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
     const int64_t slots = (int64_t)blocks * warps;
-    ensure(&d_slots_, &d_slots_cap_, (size_t)(slots * L.bytes));
+    const size_t slot_total = (size_t)(slots * L.bytes);
+    if (slot_total > d_slots_cap_) {
+        ensure(&d_slots_, &d_slots_cap_, slot_total);
+        // zeroed once: fusion stamps and slot headers start from a known state
+        cuda_check(cudaMemsetAsync(d_slots_, 0, d_slots_cap_, (cudaStream_t)stream_), "memset slots");
+    }
     stats.slots = (int32_t)slots;
     stats.slot_bytes = L.bytes;
 

@@ -228,6 +228,10 @@ def ours(args, world, rank, local, D):
     ctx = poa_b200.Context(poa_b200.Params(), device=local)
     if args.max_blocks:
         ctx.batch_config(max_blocks=args.max_blocks)
+    if args.blocks_per_sm:
+        ctx.batch_config(blocks_per_sm=args.blocks_per_sm)
+    if args.smem_per_warp:
+        ctx.batch_config(smem_per_warp=args.smem_per_warp)
 
     # ---- device-resident leg
     ctx.batch_upload(ws)
@@ -352,6 +356,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-blocks", type=int, default=0,
                     help="cap the persistent grid (small profiling captures); 0 = one full wave")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="batch kernel variant: 3 (default) or 4")
+    ap.add_argument("--smem-per-warp", type=int, default=0, help="shared memory per warp in bytes (default 16384)")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

@@ -875,27 +875,37 @@ __device__ int bt_warp_static(const RowDesc* __restrict__ desc, const int32_t* _
         const int i0 = i, a0 = acj;
         // preload: lane k -> (i0 - k, a0 - k)
         const int ri = i0 - lane, cj = a0 - lane;
-        int bsbe = 0, tbo = 0, d = 0, e0 = 0, prow0 = 0, pbase = 0;
+        int bsbe = 0, d = 0;
         uint32_t rec = 0;
         int qc = 4;
+        // predecessor row / base for the three choices a record can make (m1, m4, d)
+        int p1 = 0, b1 = 4, p4 = 0, b4 = 4, pd = 0;
         if (ri >= 0) {
             const RowDesc rd = load_desc(desc + ri);
-            bsbe = rd.bsbe; tbo = rd.tb; d = rd.d; e0 = rd.e0; prow0 = rd.prow0; pbase = rd.pbase;
+            bsbe = rd.bsbe; d = rd.d;
             const int Bs = bsbe & 0xffff, Be = bsbe >> 16;
             const int j = cj - Bs * BLK;
             if (j >= 0 && j < (Be - Bs - 1) * BLK)
-                rec = d >= 2 ? *reinterpret_cast<const uint32_t*>(tb + tbo + j * 4) : (uint32_t)tb[tbo + j];
+                rec = d >= 2 ? *reinterpret_cast<const uint32_t*>(tb + rd.tb + j * 4) : (uint32_t)tb[rd.tb + j];
             if (cj > 0) qc = qs[cj];
+            p1 = p4 = pd = rd.prow0;
+            b1 = b4 = rd.pbase;
+            if (d >= 2) {
+                const Rec r = decode_wide(rec);
+                if (r.m1 >= 0) { p1 = in_row[rd.e0 + r.m1]; b1 = in_base[rd.e0 + r.m1]; }
+                if (r.m4 >= 0) { p4 = in_row[rd.e0 + r.m4]; b4 = in_base[rd.e0 + r.m4]; }
+                if (r.dpos >= 0) pd = in_row[rd.e0 + r.dpos];
+            }
         }
         for (int t = 0; t < 32; t++) {
             const int Bs_t = __shfl_sync(0xffffffffu, bsbe, t) & 0xffff;
             const int Be_t = __shfl_sync(0xffffffffu, bsbe, t) >> 16;
             const int d_t = __shfl_sync(0xffffffffu, d, t);
-            const int e0_t = __shfl_sync(0xffffffffu, e0, t);
-            const int prow_t = __shfl_sync(0xffffffffu, prow0, t);
-            const int pbase_t = __shfl_sync(0xffffffffu, pbase, t);
             const uint32_t rec_t = __shfl_sync(0xffffffffu, rec, t);
             const int qc_t = __shfl_sync(0xffffffffu, qc, t);
+            const int p1_t = __shfl_sync(0xffffffffu, p1, t), b1_t = __shfl_sync(0xffffffffu, b1, t);
+            const int p4_t = __shfl_sync(0xffffffffu, p4, t), b4_t = __shfl_sync(0xffffffffu, b4, t);
+            const int pd_t = __shfl_sync(0xffffffffu, pd, t);
             if (acj > (Be_t - 1) * BLK || acj < Bs_t * BLK) { status = ST_BAND_ESCAPE; break; }
             const int j = acj - Bs_t * BLK;
             if (j >= (Be_t - Bs_t - 1) * BLK) { status = ST_BT_FAIL; break; }
@@ -904,13 +914,11 @@ __device__ int bt_warp_static(const RowDesc* __restrict__ desc, const int32_t* _
             int ni = i, na = acj;
             bool moved = false;
             if ((op & M_OP) && acj > 0 && r.m1 >= 0) {
-                const int p = d_t >= 2 ? in_row[e0_t + r.m1] : prow_t;
-                const int pb = d_t >= 2 ? in_base[e0_t + r.m1] : pbase_t;
-                if (lane == 0) moves[nm] = mv_pack(pb == qc_t ? MV_MATCH : MV_MISMATCH, p, qc_t);
+                if (lane == 0) moves[nm] = mv_pack(b1_t == qc_t ? MV_MATCH : MV_MISMATCH, p1_t, qc_t);
                 nm++;
-                op = ALL_OP; ni = p; na = acj - 1; moved = true;
+                op = ALL_OP; ni = p1_t; na = acj - 1; moved = true;
             } else if ((op & D_OP) && (op == D_OP || r.eqMD) && r.dpos >= 0) {
-                ni = d_t >= 2 ? in_row[e0_t + r.dpos] : prow_t;
+                ni = pd_t;
                 op = r.dext ? D_OP : (M_OP | I_OP);
                 moved = true;
             } else if ((op & I_OP) && acj > 0 && j >= 1 && (op == I_OP || r.eqMI) && (r.iopen || r.iext)) {
@@ -919,11 +927,9 @@ __device__ int bt_warp_static(const RowDesc* __restrict__ desc, const int32_t* _
                 op = r.iopen ? (M_OP | D_OP) : I_OP;
                 na = acj - 1; moved = true;
             } else if ((op & M_OP) && acj > 0 && r.m4 >= 0) {
-                const int p = d_t >= 2 ? in_row[e0_t + r.m4] : prow_t;
-                const int pb = d_t >= 2 ? in_base[e0_t + r.m4] : pbase_t;
-                if (lane == 0) moves[nm] = mv_pack(pb == qc_t ? MV_MATCH : MV_MISMATCH, p, qc_t);
+                if (lane == 0) moves[nm] = mv_pack(b4_t == qc_t ? MV_MATCH : MV_MISMATCH, p4_t, qc_t);
                 nm++;
-                op = ALL_OP; ni = p; na = acj - 1; moved = true;
+                op = ALL_OP; ni = p4_t; na = acj - 1; moved = true;
             }
             if (!moved) { status = ST_BT_FAIL; break; }
             i = ni;
@@ -1174,8 +1180,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
     __syncwarp();
 }
 
-template <int WARPS, bool STATIC>
-__global__ void __launch_bounds__(WARPS * 32, 12 / WARPS) k_batch(BatchArgs A) {
+template <int WARPS, bool STATIC, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_batch(BatchArgs A) {
     __shared__ DpArgs s_args[WARPS];
     __shared__ RowShared s_sr[WARPS];
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -1321,8 +1327,11 @@ void BatchEngine::run() {
     };
     const bool stat = p_.f > 0 && !p_.ab_band;
     if (warps != 4) throw std::invalid_argument("batch kernel is built for 4 warps per block");
-    if (stat) occ_of(k_batch<4, true>);
-    else occ_of(k_batch<4, false>);
+    // two register budgets: 3 blocks (12 warps) per SM at up to 168 registers, or
+    // 4 blocks (16 warps) per SM at up to 128 registers
+    const bool dense = blocks_per_sm >= 4;
+    if (stat) { if (dense) occ_of(k_batch<4, true, 4>); else occ_of(k_batch<4, true, 3>); }
+    else { if (dense) occ_of(k_batch<4, false, 4>); else occ_of(k_batch<4, false, 3>); }
     // every block must be resident at once (persistent kernel): never more than the occupancy allows
     const int per_sm = std::max(1, std::min(blocks_per_sm, occ));
     int blocks = sms * per_sm;
@@ -1364,8 +1373,13 @@ void BatchEngine::run() {
     A.phase = (int64_t*)(o + out_phase_);
     cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
     cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
-    if (stat) k_batch<4, true><<<blocks, 4 * 32, dyn, s>>>(A);
-    else k_batch<4, false><<<blocks, 4 * 32, dyn, s>>>(A);
+    if (stat) {
+        if (dense) k_batch<4, true, 4><<<blocks, 4 * 32, dyn, s>>>(A);
+        else k_batch<4, true, 3><<<blocks, 4 * 32, dyn, s>>>(A);
+    } else {
+        if (dense) k_batch<4, false, 4><<<blocks, 4 * 32, dyn, s>>>(A);
+        else k_batch<4, false, 3><<<blocks, 4 * 32, dyn, s>>>(A);
+    }
     cuda_check(cudaGetLastError(), "k_batch launch");
     cuda_check(cudaEventRecord((cudaEvent_t)ev1_, s), "event");
     cuda_check(cudaEventSynchronize((cudaEvent_t)ev1_), "k_batch");

@@ -649,14 +649,34 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
         }
     }
     __syncwarp();
-    // pass 3: predecessor metadata per in-edge
-    const int E = in_ptr[n];
-    for (int e = lane; e < E; e += 32) {
-        const RowMeta pm = meta[in_row[e]];
-        erec[e] = make_int4(pm.Bs | (pm.Be << 16), (int32_t)pm.st, in_w[e], in_base[e]);
+    // pass 3: each row's predecessor records in the backtrack's priority order
+    // (in_weight descending, in-list position ascending; src/align.cpp:1601,
+    // 1637, 1708 keep the first maximum), so the fill can take "the first
+    // predecessor that satisfies a test" as the backtrack's choice.
+    // erec = {Bs | Be << 16, row-store location, in_weight | position << 16,
+    //         base | (in_weight >= ind/10) << 8}
+    for (int r = lane; r < n; r += 32) {
+        const int e0 = in_ptr[r], d = r == 0 ? 0 : in_ptr[r + 1] - e0;
+        const int ind = vind[r];
+        for (int k = 0; k < d; k++) {
+            const RowMeta pm = meta[in_row[e0 + k]];
+            const int w = in_w[e0 + k];
+            const int4 rec = make_int4(pm.Bs | (pm.Be << 16), (int32_t)pm.st, (w & 0xffff) | (k << 16),
+                                       (int)in_base[e0 + k] | ((w >= ind / 10) ? 256 : 0));
+            // insertion into the sorted prefix [e0, e0 + k)
+            int at = k;
+            while (at > 0) {
+                const int4 prev = erec[e0 + at - 1];
+                const int pw = prev.z & 0xffff;
+                if (pw >= w) break;  // strictly larger weight moves ahead; ties keep list order
+                erec[e0 + at] = prev;
+                at--;
+            }
+            erec[e0 + at] = rec;
+        }
     }
     __syncwarp();
-    // pass 4: row descriptors
+    // pass 4: row descriptors (the first predecessor record is the top-priority one)
     for (int r = lane; r < n; r += 32) {
         const RowMeta rm = meta[r];
         const int e0 = in_ptr[r];
@@ -671,8 +691,8 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
         rd.prow0 = d >= 1 ? in_row[e0] : 0;
         if (d >= 1) {
             const int4 er = erec[e0];
-            rd.pbsbe = er.x; rd.pst = er.y; rd.pw = er.z; rd.pbase = er.w;
-            rd.w1ok = er.z >= rd.ind / 10;
+            rd.pbsbe = er.x; rd.pst = er.y; rd.pw = er.z & 0xffff; rd.pbase = er.w & 255;
+            rd.w1ok = (er.w >> 8) & 1;
         } else {
             rd.pbsbe = rd.pst = rd.pw = rd.pbase = 0;
             rd.w1ok = 0;
@@ -688,11 +708,21 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
 
 // Static-band DP fill of one alignment by one warp (see build_view_static).
 // Same recurrences and records as dp_fill (plain.cuh), specialised for the
-// batch: row descriptors prefetched one row ahead, the query in shared
-// memory, the previous rows' M/D in a shared-memory ring, the horizontal gap
-// recurrence in the form I[j] = o1 + (j-1)*e1 + max(K, max_{k<j} H0[k]-k*e1)
-// with K = NEG_INF + e1 - o1 (which also yields I[0] = NEG_INF), and the
-// one-byte records of single-predecessor rows built without the weight keys.
+// batch:
+//  * row descriptors and predecessor records are staged into shared memory
+//    16 rows at a time (one coalesced round trip), so the row loop reads only
+//    shared memory: descriptors, predecessor blocks from the shared-memory
+//    ring of recent rows (global spill area for rows with distant
+//    successors), the query;
+//  * the horizontal gap recurrence in the form
+//    I[j] = o1 + (j-1)*e1 + max(K, max_{k<j} H0[k]-k*e1), K = NEG_INF+e1-o1,
+//    which also yields I[0] = NEG_INF;
+//  * records: predecessors arrive in the backtrack's priority order, so each
+//    choice (M1 with its weight threshold, M4, D open / extend) is the first
+//    predecessor passing its test; single-predecessor rows keep their blocks
+//    in registers between the two passes.
+constexpr int STAGE_ROWS = 16, STAGE_EDGES = 64;
+
 __device__ __forceinline__ RowDesc load_desc(const RowDesc* p) {
     const int4* q = reinterpret_cast<const int4*>(p);
     const int4 a = q[0], b = q[1], c = q[2];
@@ -703,154 +733,205 @@ __device__ __forceinline__ RowDesc load_desc(const RowDesc* p) {
     return r;
 }
 
+__device__ __forceinline__ const int32_t* blk_src(const int32_t* ring, const int32_t* rs, int RB, int st) {
+    return st < 0 ? ring + (-st - 1) * RB * 16 : rs + st;
+}
+
 __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__ desc, const int4* __restrict__ erec,
-                                    int32_t* ring, int RB, const uint8_t* qsm, int lane) {
+                                    int32_t* ring, int RB, const uint8_t* qsm, unsigned char* stage, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
     const Scoring sc = a.sc;
     const int32_t K = add32(add32(NEG_INF, sc.e1), -sc.o1);
+    RowDesc* sdesc = reinterpret_cast<RowDesc*>(stage);
+    int4* serec = reinterpret_cast<int4*>(stage + STAGE_ROWS * sizeof(RowDesc));
     int64_t cells = 0;
-    RowDesc cur = load_desc(desc);
-    for (int i = 0; i < n; i++) {
-        RowDesc nxt;
-        if (i + 1 < n) nxt = load_desc(desc + i + 1);
-        const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
-        const int d = cur.d;
-        int32_t* dst = cur.st < 0 ? ring + (-cur.st - 1) * RB * 16 : a.rs + cur.st;
-        cells += (int64_t)bn * BLK;
-        const int nch = (bn + 31) >> 5;
-        int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
-        for (int c = 0; c < nch; c++) {
-            const int b = c * 32 + lane;
-            const bool act = b < bn;
-            const int B = Bs + b;
-            const int j0 = b * BLK;
-            int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
-            int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
-            bool c_blk = false, c_prev = false;
-            uint8_t qc8[BLK];
+    for (int i0 = 0; i0 < n; i0 += STAGE_ROWS) {
+        const int cnt = min(STAGE_ROWS, n - i0);
+        // stage: descriptors of rows i0.., and their predecessor records when they fit
+        __syncwarp();
+        if (lane < cnt * 3) {
+            const int4* src = reinterpret_cast<const int4*>(desc + i0);
+            reinterpret_cast<int4*>(sdesc)[lane] = src[lane];
+        }
+        __syncwarp();
+        const int e_lo = sdesc[0].e0;
+        const int e_hi = sdesc[cnt - 1].e0 + sdesc[cnt - 1].d;
+        const bool staged = e_hi - e_lo <= STAGE_EDGES;
+        if (staged)
+            for (int e = lane; e < e_hi - e_lo; e += 32) serec[e] = erec[e_lo + e];
+        __syncwarp();
+        const int4* er_base = staged ? serec - e_lo : erec;
+        for (int i = i0; i < i0 + cnt; i++) {
+            const RowDesc cur = sdesc[i - i0];
+            const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
+            const int d = cur.d;
+            int32_t* dst = const_cast<int32_t*>(blk_src(ring, a.rs, RB, cur.st));
+            cells += (int64_t)bn * BLK;
+            const int nch = (bn + 31) >> 5;
+            int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
+            for (int c = 0; c < nch; c++) {
+                const int b = c * 32 + lane;
+                const bool act = b < bn;
+                const int B = Bs + b;
+                const int j0 = b * BLK;
+                int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
+                int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
+                bool c_blk = false, c_prev = false;
+                uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
 #pragma unroll
-            for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
-            if (act) {
-                const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
-#pragma unroll
-                for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qw.x >> (8 * l)); qc8[4 + l] = (uint8_t)(qw.y >> (8 * l)); }
-                if (i == 0 && b == 0) Mpre[0] = 0;
-                for (int k = 0; k < d; k++) {
-                    int pbsbe, pst, pbase;
-                    if (k == 0) { pbsbe = cur.pbsbe; pst = cur.pst; pbase = cur.pbase; }
-                    else { const int4 er = erec[cur.e0 + k]; pbsbe = er.x; pst = er.y; pbase = er.w; }
-                    const int pBs = pbsbe & 0xffff, pBe = pbsbe >> 16;
-                    const int32_t* src = pst < 0 ? ring + (-pst - 1) * RB * 16 : a.rs + pst;
-                    const PredMask mk = pred_mask(B, pBs, pBe);
-                    int32_t Mb[BLK], Db[BLK];
-                    int32_t mprev = NEG_INF;
-                    if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
-                    if (mk.blk_in) {
-                        load_block16(src + (B - pBs) * 16, Mb, Db);
-                        pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
-                        if (d == 1) {
-#pragma unroll
-                            for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
-                        }
-                    }
-                    if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
-                }
-            }
-            // prefix max of the scan keys across the warp
-            int32_t key[BLK];
-            int32_t agg = INT_MIN;
-#pragma unroll
-            for (int l = 0; l < BLK; l++) {
-                H0[l] = mx(Mpre[l], Dv[l]);
-                key[l] = add32(H0[l], -(j0 + l) * sc.e1);
-                agg = mx(agg, key[l]);
-            }
-            if (!act) agg = INT_MIN;
-            const int32_t incl = warp_incl_max(agg);
-            int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
-            if (lane == 0) P = INT_MIN;
-            P = mx(P, carryP);
-            const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
-            if (i == 0) {
-#pragma unroll
-                for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
-            } else {
-                int32_t run = P;
-#pragma unroll
-                for (int l = 0; l < BLK; l++) {
-                    I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
-                    M[l] = mx(H0[l], I[l]);
-                    run = mx(run, key[l]);
-                }
-            }
-            const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
-            const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
-            const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
-            const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
-            const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
-            if (act) {
-                if (d <= 1) {
-                    uint32_t lo = 0, hi = 0;
-#pragma unroll
-                    for (int l = 0; l < BLK; l++) {
-                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                        uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
-                        if (d == 1) {
-                            const bool inr = l == 0 ? c_prev : c_blk;
-                            const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
-                            const bool bm = cur.pbase == qc8[l];
-                            const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
-                            if (eqM) r |= R_M4;
-                            if (eqM && bm && cur.w1ok) r |= R_M1;
-                            if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
-                            else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
-                        }
-                        if (l < 4) lo |= r << (8 * l);
-                        else hi |= r << (8 * (l - 4));
-                    }
-                    *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
-                } else {
-                    FlagAcc acc;
-                    flag_acc_init(acc);
+                for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
+                if (act) {
+                    const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
+                    qlo = qw.x;
+                    qhi = qw.y;
+                    if (i == 0 && b == 0) Mpre[0] = 0;
                     for (int k = 0; k < d; k++) {
-                        const int4 er = erec[cur.e0 + k];
-                        const int pBs = er.x & 0xffff, pBe = er.x >> 16;
-                        const int32_t* src = er.y < 0 ? ring + (-er.y - 1) * RB * 16 : a.rs + er.y;
+                        int pbsbe, pst, pbase;
+                        if (k == 0) { pbsbe = cur.pbsbe; pst = cur.pst; pbase = cur.pbase; }
+                        else { const int4 er = er_base[cur.e0 + k]; pbsbe = er.x; pst = er.y; pbase = er.w & 255; }
+                        const int pBs = pbsbe & 0xffff, pBe = pbsbe >> 16;
+                        const int32_t* src = blk_src(ring, a.rs, RB, pst);
                         const PredMask mk = pred_mask(B, pBs, pBe);
-                        if (!(mk.blk_in || mk.prev_in)) continue;
                         int32_t Mb[BLK], Db[BLK];
                         int32_t mprev = NEG_INF;
                         if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
-                        if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
-                        else {
+                        if (mk.blk_in) {
+                            load_block16(src + (B - pBs) * 16, Mb, Db);
+                            uint8_t qc8[BLK];
 #pragma unroll
-                            for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                            for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qlo >> (8 * l)); qc8[4 + l] = (uint8_t)(qhi >> (8 * l)); }
+                            pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+                            if (d == 1) {
+#pragma unroll
+                                for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
+                            }
                         }
-                        flags_pred(sc, mk, er.w, er.z, k, Mb, Db, mprev, qc8, M, Dv, acc);
+                        if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
                     }
-                    uint32_t r[BLK];
+                }
+                // prefix max of the scan keys across the warp
+                int32_t agg = INT_MIN;
+#pragma unroll
+                for (int l = 0; l < BLK; l++) {
+                    H0[l] = mx(Mpre[l], Dv[l]);
+                    agg = mx(agg, add32(H0[l], -(j0 + l) * sc.e1));
+                }
+                if (!act) agg = INT_MIN;
+                const int32_t incl = warp_incl_max(agg);
+                int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
+                if (lane == 0) P = INT_MIN;
+                P = mx(P, carryP);
+                const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
+                if (i == 0) {
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
+                } else {
+                    int32_t run = P;
 #pragma unroll
                     for (int l = 0; l < BLK; l++) {
-                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                        r[l] = encode_wide(own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il), acc, l, cur.ind);
+                        I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
+                        M[l] = mx(H0[l], I[l]);
+                        run = mx(run, add32(H0[l], -(j0 + l) * sc.e1));
                     }
-                    uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
-                    tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
-                    tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
                 }
-                store_block16(dst + b * 16, M, Dv);
+                const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
+                const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
+                const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
+                const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
+                const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
+                if (act) {
+                    if (d <= 1) {
+                        uint32_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) {
+                            const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                            uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
+                            if (d == 1) {
+                                const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
+                                const bool inr = l == 0 ? c_prev : c_blk;
+                                const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
+                                const bool bm = cur.pbase == qc;
+                                const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                                if (eqM) r |= R_M4;
+                                if (eqM && bm && cur.w1ok) r |= R_M1;
+                                if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
+                                else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
+                            }
+                            if (l < 4) lo |= r << (8 * l);
+                            else hi |= r << (8 * (l - 4));
+                        }
+                        *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
+                    } else {
+                        // choices per cell: m1 | m4 << 16, dopen | dext << 16 (511 = none,
+                        // 510 = the best matching predecessor failed the weight threshold)
+                        uint32_t cm[BLK], cd[BLK];
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) { cm[l] = 0x01ff01ffu; cd[l] = 0x01ff01ffu; }
+                        for (int k = 0; k < d; k++) {
+                            const int4 er = er_base[cur.e0 + k];
+                            const int pBs = er.x & 0xffff, pBe = er.x >> 16;
+                            const int32_t* src = blk_src(ring, a.rs, RB, er.y);
+                            const PredMask mk = pred_mask(B, pBs, pBe);
+                            if (!(mk.blk_in || mk.prev_in)) continue;
+                            const uint32_t pos = (uint32_t)er.z >> 16;
+                            const int pbase = er.w & 255;
+                            const uint32_t m1v = (er.w & 256) ? pos : 510u;
+                            int32_t Mb[BLK], Db[BLK];
+                            int32_t mprev = NEG_INF;
+                            if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                            if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
+                            else {
+#pragma unroll
+                                for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                            }
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) {
+                                const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
+                                const bool inr = l == 0 ? mk.prev_in : mk.blk_in;
+                                const int32_t mv = l == 0 ? mprev : Mb[l > 0 ? l - 1 : 0];
+                                const bool bm = pbase == qc;
+                                const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                                if (eqM && (cm[l] >> 16) == 511u) cm[l] = (cm[l] & 0xffffu) | (pos << 16);
+                                if (eqM && bm && (cm[l] & 0xffffu) == 511u) cm[l] = (cm[l] & 0xffff0000u) | m1v;
+                                if (mk.blk_in) {
+                                    if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
+                                        cd[l] = (cd[l] & 0xffff0000u) | pos;
+                                    if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
+                                        cd[l] = (cd[l] & 0xffffu) | (pos << 16);
+                                }
+                            }
+                        }
+                        uint32_t r[BLK];
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) {
+                            const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                            uint32_t w = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
+                            uint32_t m1 = cm[l] & 0xffffu, m4 = cm[l] >> 16;
+                            if (m1 == 510u) m1 = W_NONE;
+                            uint32_t dd = cd[l] & 0xffffu;
+                            if (dd == 511u) {
+                                dd = cd[l] >> 16;
+                                if (dd != 511u) w |= W_DEXT;
+                            }
+                            r[l] = w | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
+                        }
+                        uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
+                        tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
+                        tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
+                    }
+                    store_block16(dst + b * 16, M, Dv);
+                }
+                carryP = mx(carryP, chunk_total);
+                carryM = nextM;
+                carryI = nextI;
             }
-            carryP = mx(carryP, chunk_total);
-            carryM = nextM;
-            carryI = nextI;
+            __syncwarp();
         }
-        cur = nxt;
-        __syncwarp();
     }
     if (lane == 0) {
         const RowMeta last = a.meta[n - 1];
         const int jm = m - last.Bs * BLK;
-        const int32_t* src = last.st < 0 ? ring + (int64_t)(-last.st - 1) * RB * 16 : a.rs + last.st;
+        const int32_t* src = blk_src(ring, a.rs, RB, (int)last.st);
         a.out[1] = src[(jm / BLK) * 16 + jm % BLK];
         a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
         a.out[0] = ST_OK;
@@ -1114,8 +1195,9 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             for (int64_t x = lane * 16; x < qsb; x += 32 * 16)
                 *reinterpret_cast<uint4*>(qsm + x) = *reinterpret_cast<const uint4*>(qs + x);
             __syncwarp();
+            unsigned char* stage = qsm + ((qsb + 15) & ~(int64_t)15);
             dp_fill_warp_static(a, (const RowDesc*)(s + L.v_desc), (const int4*)(s + L.v_pmeta), (int32_t*)wsm,
-                                A.sring_blocks, qsm, lane);
+                                A.sring_blocks, qsm, stage, lane);
         } else {
             dp_fill(grp, a);
         }
@@ -1316,9 +1398,10 @@ void BatchEngine::run() {
     // static band: shared-memory ring of up to 8 rows of ring_blocks blocks
     int sring_blocks = ring_blocks;
     const int qsm_bytes = (int)((qs_bytes(QC) + 15) / 16 * 16);
-    int sring_rows = std::min(8, (smem_w - qsm_bytes) / std::max(1, sring_blocks * 64));
+    const int stage_bytes = STAGE_ROWS * (int)sizeof(RowDesc) + STAGE_EDGES * 16;
+    int sring_rows = std::min(8, (smem_w - qsm_bytes - stage_bytes) / std::max(1, sring_blocks * 64));
     if (sring_rows < 2) sring_rows = 0;
-    if (p_.f > 0 && !p_.ab_band && qsm_bytes > smem_w)
+    if (p_.f > 0 && !p_.ab_band && qsm_bytes + stage_bytes > smem_w)
         throw std::invalid_argument("reads too long for the batch kernel's shared memory; raise smem_per_warp");
     int occ = 0;
     auto occ_of = [&](auto kern) {

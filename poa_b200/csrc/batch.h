@@ -53,7 +53,7 @@ class BatchEngine {
     BatchStats stats;
     int32_t warps_per_block = 4;
     int32_t blocks_per_sm = 3;  // 3: 168-register build; >= 4: 128-register build (occupancy still caps it)
-    int32_t smem_per_warp = 16384;  // shared-memory row ring / topsort workspace per warp
+    int32_t smem_per_warp = 18432;  // shared-memory row ring + staging / topsort workspace per warp
     int32_t max_blocks = 0;         // cap on the persistent grid (0 = one wave of resident blocks)
 
   private:

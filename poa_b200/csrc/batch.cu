@@ -749,9 +749,9 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         const int cnt = min(STAGE_ROWS, n - i0);
         // stage: descriptors of rows i0.., and their predecessor records when they fit
         __syncwarp();
-        if (lane < cnt * 3) {
+        {
             const int4* src = reinterpret_cast<const int4*>(desc + i0);
-            reinterpret_cast<int4*>(sdesc)[lane] = src[lane];
+            for (int x = lane; x < cnt * 3; x += 32) reinterpret_cast<int4*>(sdesc)[x] = src[x];
         }
         __syncwarp();
         const int e_lo = sdesc[0].e0;

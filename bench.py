@@ -52,6 +52,16 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def shard_seed(rank: int) -> int:
+    """Seed of rank r's windows: every rank runs its own 20,000 windows (weak scaling)."""
+    return 4 + 1000 * rank
+
+
+def whole_job_rate(world: int, units_per_rank: int, steps: int, t_max: float) -> float:
+    """Units per second over all ranks, timed by the slowest rank."""
+    return world * units_per_rank * steps / t_max
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rk = int(os.environ.get("RANK", "0"))
@@ -218,7 +228,7 @@ def ours(args, world, rank, local, D):
     import poa_b200
     from poa_b200 import synth
     t0 = time.perf_counter()
-    ws = synth.polishing_windows(seed=4 + 1000 * rank, n_windows=args.windows)
+    ws = synth.polishing_windows(seed=shard_seed(rank), n_windows=args.windows)
     log(f"[rank {rank}] generated {ws.n_windows} windows / {ws.n_reads} reads in {time.perf_counter() - t0:.1f}s")
     try:
         import torch
@@ -269,14 +279,14 @@ def ours(args, world, rank, local, D):
         D.barrier()
         t_e2e = D.max(time.perf_counter() - t0)
         st2 = ctx.batch_stats()
-        e2e = {"value": world * ws.n_windows * args.steps / t_e2e, "unit": "windows/s",
+        e2e = {"value": whole_job_rate(world, ws.n_windows, args.steps, t_e2e), "unit": "windows/s",
                "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
                "ms_per_step": 1e3 * t_e2e / args.steps, "api": "poa_batch_consensus"}
         assert c2 == cons and s2 == status, "end-to-end run disagrees with the device-resident run"
         for h in holders:
             h.close()
 
-    value = world * ws.n_windows * args.steps / t_dev
+    value = whole_job_rate(world, ws.n_windows, args.steps, t_dev)
     kernel_s = t_dev / args.steps
     peaks = load_peaks()
     achieved = cells * BYTES_PER_CELL / kernel_s / 1e9

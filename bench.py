@@ -250,8 +250,10 @@ def ours(args, world, rank, local, D):
     D.barrier()
     clk = ClockSampler(gpu_uuid(local))
     dev_ms = []
+    launches = 0
     for _ in range(args.steps):
         dev_ms.append(ctx.batch_run())
+        launches += ctx.batch_stats()["launches"]
     D.barrier()
     clocks = clk.stop()
     st = ctx.batch_stats()
@@ -305,7 +307,7 @@ def ours(args, world, rank, local, D):
                    "l2": "inputs (%.0f MB) larger than L2 (126 MB)" % (ws.seq.shape[0] / 1e6)},
         "gcups": world * cells * args.steps / t_dev / 1e9,
         "cells_per_step": cells, "failed_windows": failed,
-        "gpu_launches": args.steps, "e2e": e2e, "roofline": roofline, "clocks": clocks,
+        "gpu_launches": launches, "retried_windows": st["retried"], "e2e": e2e, "roofline": roofline, "clocks": clocks,
         "slots": st["slots"], "slot_bytes": st["slot_bytes"],
         "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
         "phase_mcycles_per_window": {k: v / 1e6 / ws.n_windows for k, v in st["phase_cycles"].items()},

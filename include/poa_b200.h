@@ -132,8 +132,10 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
 /* [0] band cells of the last run, [1] windows that failed, [2] concurrent
  * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes,
  * [6..11] summed per-window clock cycles of the view build, DP fill,
- * backtrack, graph fusion, topological sort and consensus phases. */
-int poa_batch_stats(poa_ctx* ctx, int64_t* out12);
+ * backtrack, graph fusion, topological sort and consensus phases,
+ * [12] kernel launches of the last run, [13] windows re-run with larger
+ * capacities. */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out14);
 
 /* One poa() alignment on inputs already in device memory, without
  * allocating anything (no counterpart in the reference).

@@ -236,11 +236,11 @@ class Context:
                 self._check(lib().poa_batch_config(self._h, key, int(val)))
 
     def batch_stats(self) -> dict:
-        o = (ctypes.c_int64 * 12)()
+        o = (ctypes.c_int64 * 14)()
         self._check(lib().poa_batch_stats(self._h, o))
         names = ("view", "fill", "backtrack", "fusion", "topsort", "consensus")
         return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5],
-                    phase_cycles={names[k]: o[6 + k] for k in range(6)})
+                    phase_cycles={names[k]: o[6 + k] for k in range(6)}, launches=o[12], retried=o[13])
 
     def set_timing(self, on: bool = True):
         lib().poa_set_timing(self._h, 1 if on else 0)

@@ -1374,13 +1374,37 @@ void BatchEngine::upload(const BatchInput& in, const Params& p) {
 
 void BatchEngine::run() {
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    stats.kernel_ms = 0.0;
+    stats.retried = 0;
+    stats.launches = 0;
+    // first pass over every window; windows that outgrow their slot (ST_CAPACITY /
+    // ST_OOM) are re-run with doubled capacities, up to three times
+    launch(order_.data(), n_windows_, 1);
+    for (int attempt = 2; attempt <= 8; attempt *= 2) {
+        cudaStream_t s = (cudaStream_t)stream_;
+        char* h = (char*)h_out_;
+        cuda_check(cudaMemcpyAsync(h + out_status_, (char*)d_out_ + out_status_, 4 * (size_t)n_windows_,
+                                   cudaMemcpyDeviceToHost, s), "D2H status");
+        cuda_check(cudaStreamSynchronize(s), "D2H status");
+        const int32_t* st = (const int32_t*)(h + out_status_);
+        std::vector<int32_t> redo;
+        for (int w = 0; w < n_windows_; w++)
+            if (st[w] == ST_CAPACITY || st[w] == ST_OOM) redo.push_back(w);
+        if (redo.empty()) break;
+        stats.retried += (int32_t)redo.size();
+        launch(redo.data(), (int32_t)redo.size(), attempt);
+    }
+}
+
+void BatchEngine::launch(const int32_t* windows, int32_t count, int scale) {
     cudaStream_t s = (cudaStream_t)stream_;
     int sms = 0;
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attr");
     const bool adaptive = p_.f > 0 && p_.ab_band;
-    // capacities from the data (a window beyond them reports ST_CAPACITY / ST_OOM)
-    const int64_t NC64 = std::min<int64_t>(2 + max_win_bases_, 2 + 8 * (int64_t)max_len_ + 256);
-    const int32_t NC = (int32_t)NC64;
+    // capacities from the data, scaled on retries
+    const int64_t est = 2 + (int64_t)max_len_ + (int64_t)(0.2 * (double)max_win_bases_) + 256;
+    const int64_t NC64 = std::min<int64_t>(std::min<int64_t>(2 + max_win_bases_, est * scale), 60000);
+    const int32_t NC = (int32_t)std::max<int64_t>(NC64, 64);
     const int32_t EC = 3 * NC;
     const int32_t QC = max_len_ + 8;
     const int m = max_len_ + 1;
@@ -1388,9 +1412,10 @@ void BatchEngine::run() {
     int ring_blocks = p_.f > 0 ? std::min(m / BLK + 2, (2 * wb) / BLK + 4) : m / BLK + 2;
     if (adaptive) ring_blocks = std::min(m / BLK + 2, (4 * wb) / BLK + 4);
     ring_blocks = std::max(ring_blocks, 4);
+    const int tb_blocks = adaptive ? std::min(m / BLK + 2, ring_blocks * scale) : ring_blocks;
     const int32_t ring_rows = 32;
-    const int64_t spill_rows = std::max<int64_t>(NC / 4, 64);
-    const int64_t tb_cap = (int64_t)NC * ring_blocks * BLK * 2 + 4096;
+    const int64_t spill_rows = std::min<int64_t>(NC, std::max<int64_t>(NC / 4, 64) * scale);
+    const int64_t tb_cap = (int64_t)NC * tb_blocks * BLK * 2 * std::min(scale, 2) + 4096;
     SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill_rows, tb_cap, adaptive);
     const int warps = warps_per_block;
     const int smem_w = smem_per_warp;
@@ -1419,18 +1444,36 @@ void BatchEngine::run() {
     const int per_sm = std::max(1, std::min(blocks_per_sm, occ));
     int blocks = sms * per_sm;
     if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
+    // and the slots must fit the device-memory budget (75 % of what is free, counting our own slots)
+    size_t free_b = 0, total_b = 0;
+    cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t budget = (size_t)(0.75 * (double)(free_b + d_slots_cap_));
+    const int64_t max_by_mem = (int64_t)(budget / (size_t)L.bytes) / warps;
+    if (max_by_mem < 1) throw std::runtime_error("not enough device memory for one batch slot");
+    blocks = (int)std::min<int64_t>(blocks, max_by_mem);
+    blocks = std::min(blocks, (count + warps - 1) / warps);
+    blocks = std::max(blocks, 1);
     const int64_t slots = (int64_t)blocks * warps;
     const size_t slot_total = (size_t)(slots * L.bytes);
     if (slot_total > d_slots_cap_) {
-        ensure(&d_slots_, &d_slots_cap_, slot_total);
+        if (d_slots_) cuda_check(cudaFree(d_slots_), "cudaFree");
+        d_slots_ = nullptr;
+        d_slots_cap_ = 0;
+        cuda_check(cudaMalloc(&d_slots_, slot_total), "cudaMalloc(batch slots)");
+        d_slots_cap_ = slot_total;
         // zeroed once: fusion stamps and slot headers start from a known state
-        cuda_check(cudaMemsetAsync(d_slots_, 0, d_slots_cap_, (cudaStream_t)stream_), "memset slots");
+        cuda_check(cudaMemsetAsync(d_slots_, 0, d_slots_cap_, s), "memset slots");
     }
     stats.slots = (int32_t)slots;
     stats.slot_bytes = L.bytes;
 
     char* d = (char*)d_in_;
     char* o = (char*)d_out_;
+    if (windows != order_.data() || count != n_windows_)
+        cuda_check(cudaMemcpyAsync(d + off_order_, windows, 4 * (size_t)count, cudaMemcpyHostToDevice, s), "H2D order");
+    else
+        cuda_check(cudaMemcpyAsync(d + off_order_, order_.data(), 4 * (size_t)count, cudaMemcpyHostToDevice, s),
+                   "H2D order");
     BatchArgs A;
     A.seq = (const uint8_t*)(d + off_seq_);
     A.read_off = (const int64_t*)(d + off_roff_);
@@ -1438,7 +1481,7 @@ void BatchEngine::run() {
     A.win_off = (const int32_t*)(d + off_woff_);
     A.order = (const int32_t*)(d + off_order_);
     A.counter = (int32_t*)(d + off_ctr_);
-    A.n_windows = n_windows_;
+    A.n_windows = count;
     A.sc = scoring_of(p_);
     A.b = p_.b;
     A.f = p_.f;
@@ -1468,7 +1511,8 @@ void BatchEngine::run() {
     cuda_check(cudaEventSynchronize((cudaEvent_t)ev1_), "k_batch");
     float ms = 0.f;
     cuda_check(cudaEventElapsedTime(&ms, (cudaEvent_t)ev0_, (cudaEvent_t)ev1_), "elapsed");
-    stats.kernel_ms = ms;
+    stats.kernel_ms += ms;
+    stats.launches++;
 }
 
 void BatchEngine::sync_stats() {

@@ -33,6 +33,7 @@ struct BatchStats {
     int64_t h2d_bytes = 0, d2h_bytes = 0;
     int32_t failed = 0;       // windows that ended with a non-OK status
     int32_t retried = 0;      // windows re-run with larger capacities
+    int32_t launches = 0;     // kernel launches of the last run()
     // summed lane-0 clock cycles per phase over all windows: view build, DP
     // fill, backtrack, fusion, topological sort, consensus
     int64_t phase_cycles[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -58,6 +59,8 @@ class BatchEngine {
 
   private:
     void ensure(void** ptr, size_t* cap, size_t bytes);
+    // one persistent launch over `count` windows (ids), capacities scaled by `scale`
+    void launch(const int32_t* windows, int32_t count, int scale);
     int device_;
     void* stream_ = nullptr;
     void* ev0_ = nullptr;

@@ -307,6 +307,8 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
     const pb::BatchStats& s = ctx->batch->stats;
     o[0] = s.cells; o[1] = s.failed; o[2] = s.slots; o[3] = s.slot_bytes; o[4] = s.h2d_bytes; o[5] = s.d2h_bytes;
     for (int k = 0; k < 6; k++) o[6 + k] = s.phase_cycles[k];
+    o[12] = s.launches;
+    o[13] = s.retried;
     return POA_OK;
 }
 

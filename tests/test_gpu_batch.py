@@ -84,3 +84,43 @@ def test_batch_vs_oracle(oracle_bin, tmp_path):
         want = subprocess.run([oracle_bin, str(fa)], capture_output=True, check=True).stdout
         assert st[w] == 0
         assert cons[w] == _cons_of(want), w
+
+
+def test_batch_learned_band_config_windows(oracle_bin, tmp_path):
+    """2,000 bp windows, 15 % error, 20-24 reads, adaptive band (-B), 1 chimeric
+    read in 10: the configuration the learned band proposer works on."""
+    ws = synth.windows(41, 3, (2000, 2000), (20, 24), 0.15, chimeric=0.1)
+    with poa_b200.Context(poa_b200.Params(ab_band=True)) as ctx:
+        ctx.batch_upload(ws)
+        ctx.batch_run()
+        cons, st = ctx.batch_download()
+    for w in range(ws.n_windows):
+        fa = tmp_path / f"w{w}.fa"
+        synth.write_fasta(str(fa), ws.window_reads(w))
+        want = subprocess.run([oracle_bin, str(fa), "-B"], capture_output=True, check=True, timeout=600).stdout
+        assert st[w] == 0
+        assert cons[w] == _cons_of(want), w
+
+
+def test_batch_capacity_retry():
+    """A window far larger than the rest outgrows the slot sized from the batch
+    statistics at first; the engine re-runs it with larger capacities and the
+    result is still the reference's."""
+    small = synth.windows(42, 30, (300, 300), (4, 6), 0.08)
+    big = synth.windows(43, 1, (600, 600), (60, 60), 0.25)
+    reads, offs = [], [0]
+    for w in range(small.n_windows):
+        reads += small.window_reads(w)
+        offs.append(len(reads))
+    reads += big.window_reads(0)
+    offs.append(len(reads))
+    ws = synth.pack_windows_from_reads(reads, offs)
+    with poa_b200.Context() as ctx:
+        ctx.batch_upload(ws)
+        ctx.batch_run()
+        cons, st = ctx.batch_download()
+        stats = ctx.batch_stats()
+    assert all(x == 0 for x in st)
+    solo = poa_b200.run(big.window_reads(0))
+    assert b">consensus sequence\n" + cons[-1] + b"\n" == solo
+    print("retried", stats["retried"], "launches", stats["launches"])

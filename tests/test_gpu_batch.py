@@ -107,7 +107,7 @@ def test_batch_capacity_retry():
     statistics at first; the engine re-runs it with larger capacities and the
     result is still the reference's."""
     small = synth.windows(42, 30, (300, 300), (4, 6), 0.08)
-    big = synth.windows(43, 1, (600, 600), (60, 60), 0.25)
+    big = synth.windows(43, 1, (600, 600), (60, 60), 0.40)
     reads, offs = [], [0]
     for w in range(small.n_windows):
         reads += small.window_reads(w)

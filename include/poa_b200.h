@@ -134,8 +134,27 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * [6..11] summed per-window clock cycles of the view build, DP fill,
  * backtrack, graph fusion, topological sort and consensus phases,
  * [12] kernel launches of the last run, [13] windows re-run with larger
- * capacities. */
-int poa_batch_stats(poa_ctx* ctx, int64_t* out14);
+ * capacities, [14] windows that outgrew the plan's sizing (poa_batch_plan)
+ * and were re-run with the default sizing, [15] device time of the last run
+ * in microseconds. */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out16);
+/* Resource plan for the uploaded windows (no counterpart in the reference:
+ * the reference allocates per alignment). One value per window: graph nodes,
+ * traceback record bytes and spilled row-store entries (int32) of its
+ * largest alignment, and a relative cost; typically a band proposer's
+ * prediction from poa_batch_read_stats-style targets. The plan sizes the
+ * device slots and orders the windows (largest cost first); it never changes
+ * a band, so results are the same with or without it. A window that
+ * outgrows its slot is re-run with the default sizing. nodes == NULL clears
+ * the plan; poa_batch_upload clears it too. */
+int poa_batch_plan(poa_ctx* ctx, const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill,
+                   const float* cost);
+/* Per read of the last run, 8 values each (n_reads * 8 entries): widest DP
+ * row in 8-column blocks, band cells, DP rows, graph nodes after fusing the
+ * read, traceback record bytes, spilled row-store entries (int32), graph
+ * edges after fusing the read, 0. A window's first read has no DP: its DP
+ * values are zero. These are the band statistics the band proposer learns. */
+int poa_batch_read_stats(poa_ctx* ctx, int32_t* out, int64_t cap);
 
 /* One poa() alignment on inputs already in device memory, without
  * allocating anything (no counterpart in the reference).

@@ -117,6 +117,8 @@ def lib() -> ctypes.CDLL:
     L.poa_batch_stats.argtypes = [ctypes.c_void_p, _i64p]
     L.poa_set_timing.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.poa_batch_config.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
+    L.poa_batch_read_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+    L.poa_batch_plan.argtypes = [ctypes.c_void_p] * 5
     L.poa_alloc_pinned.restype = ctypes.c_void_p
     L.poa_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
@@ -229,6 +231,15 @@ class Context:
         raw = cons.raw
         return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
 
+    def batch_read_stats(self):
+        """int32 array [n_reads, 8] of the last run: widest row (blocks), cells, rows,
+        nodes after fusion, record bytes, spilled row-store entries, edges after fusion, 0."""
+        import numpy as np
+        n = int(self._keep[2].shape[0]) if getattr(self, "_keep", None) is not None else 0
+        out = np.zeros((max(n, 1), 8), dtype=np.int32)
+        self._check(lib().poa_batch_read_stats(self._h, out.ctypes.data, out.size))
+        return out[:n]
+
     def batch_config(self, blocks_per_sm=None, max_blocks=None, smem_per_warp=None):
         """Launch shape of the batch kernel (see poa_batch_config)."""
         for key, val in ((0, blocks_per_sm), (1, max_blocks), (2, smem_per_warp)):
@@ -236,11 +247,26 @@ class Context:
                 self._check(lib().poa_batch_config(self._h, key, int(val)))
 
     def batch_stats(self) -> dict:
-        o = (ctypes.c_int64 * 14)()
+        o = (ctypes.c_int64 * 16)()
         self._check(lib().poa_batch_stats(self._h, o))
         names = ("view", "fill", "backtrack", "fusion", "topsort", "consensus")
         return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5],
-                    phase_cycles={names[k]: o[6 + k] for k in range(6)}, launches=o[12], retried=o[13])
+                    phase_cycles={names[k]: o[6 + k] for k in range(6)}, launches=o[12], retried=o[13],
+                    fallback=o[14], kernel_us=o[15])
+
+    def batch_plan(self, nodes=None, tb_bytes=None, spill=None, cost=None):
+        """Per-window resource plan (see poa_batch_plan); no arguments clears it."""
+        import numpy as np
+        if nodes is None:
+            self._check(lib().poa_batch_plan(self._h, None, None, None, None))
+            return
+        n = np.ascontiguousarray(nodes, dtype=np.int32)
+        t = np.ascontiguousarray(tb_bytes, dtype=np.int64)
+        sp = np.ascontiguousarray(spill, dtype=np.int64)
+        c = np.ascontiguousarray(cost, dtype=np.float32)
+        if not (n.shape[0] == t.shape[0] == sp.shape[0] == c.shape[0] == self._nwin):
+            raise ValueError("plan arrays need one value per uploaded window")
+        self._check(lib().poa_batch_plan(self._h, n.ctypes.data, t.ctypes.data, sp.ctypes.data, c.ctypes.data))
 
     def set_timing(self, on: bool = True):
         lib().poa_set_timing(self._h, 1 if on else 0)

@@ -41,12 +41,12 @@ struct SlotLayout {
     int64_t bytes;
 };
 
-SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, int32_t ring_blocks, int64_t spill_rows,
+SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, int32_t ring_blocks, int64_t spill,
                        int64_t tb_cap, bool adaptive) {
     SlotLayout L;
     L.NC = NC; L.EC = EC; L.QC = QC;
     L.ring_rows = ring_rows; L.ring_blocks = ring_blocks;
-    L.rs_cap = (int64_t)ring_rows * ring_blocks * 16 + spill_rows * ring_blocks * 16;
+    L.rs_cap = (int64_t)ring_rows * ring_blocks * 16 + spill;
     L.tb_cap = tb_cap;
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t r = o; o = up256(o + bytes); return (int64_t)r; };
@@ -96,6 +96,7 @@ struct BatchArgs {
     int32_t* status;
     int64_t* cells;
     int64_t* phase;  // [n_windows * NPHASE] lane-0 clock cycles per phase
+    int32_t* rstats; // [n_reads * NRSTAT] per read, see BatchEngine::read_stats
 };
 
 // per-window cycle counters (clock64 on lane 0): where a window's time goes
@@ -103,7 +104,7 @@ enum { PH_VIEW = 0, PH_FILL, PH_BT, PH_FUSE, PH_SORT, PH_CONS, NPHASE = 8 };
 
 // Pointers of one slot's device graph.
 struct DevGraph {
-    int32_t* hdr;  // [0] nodes, [1] edges
+    int32_t* hdr;  // [0] nodes, [1] edges, [2] status, [3] ranks, [4..11] DP outputs, [12] fusion stamp, [13] moves
     uint8_t* base;
     int32_t *par, *aligned, *ind, *rank, *in_head, *in_tail, *out_head, *out_tail, *in_cnt, *out_cnt;
     int32_t *e_from, *e_to, *e_w, *e_nin, *e_nout;
@@ -631,6 +632,10 @@ __device__ int build_view_static(DevGraph& g, char* s, const SlotLayout& L, WinV
         ci_c += __shfl_sync(0xffffffffu, xi, 31);
         tb_c += __shfl_sync(0xffffffffu, xt, 31);
         sp_c += __shfl_sync(0xffffffffu, xs, 31);
+    }
+    if (lane == 0) {
+        g.hdr[8] = (int32_t)(tb_c > INT_MAX ? INT_MAX : tb_c);   // DP output 4: record bytes
+        g.hdr[9] = (int32_t)(sp_c > INT_MAX ? INT_MAX : sp_c);   // DP output 5: spilled row-store entries
     }
     if (__any_sync(0xffffffffu, bad)) return ST_DEGENERATE;
     if (tb_c > L.tb_cap || sp_c > spill_cap) return ST_OOM;
@@ -1202,6 +1207,29 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             dp_fill(grp, a);
         }
         __syncwarp();
+        {
+            // per-read band statistics
+            int mbn = 0;
+            for (int i = lane; i < v.n; i += 32) {
+                const RowMeta rm = ((const RowMeta*)(s + L.meta))[i];
+                mbn = max(mbn, rm.Be - rm.Bs - 1);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mbn = max(mbn, __shfl_xor_sync(0xffffffffu, mbn, o));
+            if (lane == 0) {
+                int32_t* o = A.rstats + (int64_t)r * NRSTAT;
+                o[0] = mbn;
+                o[1] = a.out[3];
+                o[2] = v.n;
+                if constexpr (static_band) {
+                    o[4] = a.out[4];  // record bytes and spilled row-store entries (view scan)
+                    o[5] = a.out[5];
+                } else {
+                    o[4] = (int32_t)sr->tb_next;
+                    o[5] = (int32_t)(sr->st_next - (int64_t)L.ring_rows * L.ring_blocks * 16);
+                }
+            }
+        }
         tick(PH_FILL);
         if constexpr (static_band) {
             int st = a.out[0];
@@ -1212,8 +1240,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             if (lane == 0) {
                 cells += a.out[3];
                 g.hdr[2] = st;
-                g.hdr[9] = nm;
-                g.hdr[8] = g.hdr[8] + 1;  // fusion stamp, increasing over the slot's lifetime
+                g.hdr[13] = nm;
+                g.hdr[12] = g.hdr[12] + 1;  // fusion stamp, increasing over the slot's lifetime
             }
         } else if (lane == 0) {
             int st = a.out[0];
@@ -1221,16 +1249,16 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             int32_t nm = 0;
             if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
             g.hdr[2] = st;
-            g.hdr[9] = nm;
-            g.hdr[8] = g.hdr[8] + 1;
+            g.hdr[13] = nm;
+            g.hdr[12] = g.hdr[12] + 1;
         }
         __syncwarp();
         tick(PH_BT);
         {
             int st = g.hdr[2];
-            const int nm = g.hdr[9];
+            const int nm = g.hdr[13];
             if (st == ST_OK) {
-                st = dg_fuse_warp(g, a.moves, nm, beg_i, (int32_t*)(s + L.path), g.hdr[8], lane);
+                st = dg_fuse_warp(g, a.moves, nm, beg_i, (int32_t*)(s + L.path), g.hdr[12], lane);
                 if (st == -1) {
                     // sequential fusion (a path that repeats a node or an aligned sibling)
                     st = ST_OK;
@@ -1242,6 +1270,10 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         }
         __syncwarp();
         status = g.hdr[2];
+        if (lane == 0) {
+            A.rstats[(int64_t)r * NRSTAT + 3] = g.hdr[0];
+            A.rstats[(int64_t)r * NRSTAT + 6] = g.hdr[1];
+        }
         tick(PH_FUSE);
         if (status == ST_OK && r + 1 < r1)
             dg_topsort_warp(g, g.hdr[0], g.hdr[1], lens, (uint16_t*)wsm, A.smem_per_warp, lane);
@@ -1319,6 +1351,7 @@ void BatchEngine::upload(const BatchInput& in, const Params& p) {
     if (p.enable_seeding || p.progressive || p.result != 0)
         throw std::invalid_argument("batched windows support the consensus mode without -S/-p");
     p_ = p;
+    set_plan(nullptr, nullptr, nullptr, nullptr);
     n_windows_ = in.n_windows;
     n_reads_ = in.n_reads;
     max_len_ = 0;
@@ -1361,6 +1394,7 @@ void BatchEngine::upload(const BatchInput& in, const Params& p) {
     out_status_ = o; o = up256(o + 4 * (size_t)n_windows_);
     out_cells_ = o; o = up256(o + 8 * (size_t)n_windows_);
     out_phase_ = o; o = up256(o + 8 * (size_t)NPHASE * n_windows_);
+    out_rstats_ = o; o = up256(o + 4 * (size_t)NRSTAT * n_reads_);
     out_bytes_ = o;
     ensure(&d_out_, &d_out_cap_, o);
     if (h_out_cap_ < o) {
@@ -1377,10 +1411,33 @@ void BatchEngine::run() {
     stats.kernel_ms = 0.0;
     stats.retried = 0;
     stats.launches = 0;
-    // first pass over every window; windows that outgrow their slot (ST_CAPACITY /
-    // ST_OOM) are re-run with doubled capacities, up to three times
-    launch(order_.data(), n_windows_, 1);
-    for (int attempt = 2; attempt <= 8; attempt *= 2) {
+    if (n_reads_ > 0)
+        cuda_check(cudaMemsetAsync((char*)d_out_ + out_rstats_, 0, 4 * (size_t)NRSTAT * n_reads_, (cudaStream_t)stream_),
+                   "memset read stats");
+    stats.fallback = 0;
+    // With a plan, one pass sized by the plan's largest window, in the plan's
+    // cost order; its windows that outgrow their slot fall back to the sizing
+    // below. Without one, a first pass with capacities estimated from the read
+    // lengths. Windows that outgrow their slot (ST_CAPACITY / ST_OOM) are re-run
+    // with doubled capacities, up to three times.
+    int first = 1;
+    if (!plan_nodes_.empty()) {
+        Caps c;
+        c.NC = 64;
+        c.tb_cap = 4096;
+        c.spill = 0;
+        for (int w = 0; w < n_windows_; w++) {
+            c.NC = std::max<int64_t>(c.NC, plan_nodes_[w]);
+            c.tb_cap = std::max(c.tb_cap, plan_tb_[w]);
+            c.spill = std::max(c.spill, plan_spill_[w]);
+        }
+        c.NC = std::min<int64_t>(c.NC, 60000);
+        launch(plan_order_.data(), n_windows_, c);
+        first = 0;
+    } else {
+        launch(order_.data(), n_windows_, default_caps(1));
+    }
+    for (int attempt = first ? 2 : 1; attempt <= 8; attempt *= 2) {
         cudaStream_t s = (cudaStream_t)stream_;
         char* h = (char*)h_out_;
         cuda_check(cudaMemcpyAsync(h + out_status_, (char*)d_out_ + out_status_, 4 * (size_t)n_windows_,
@@ -1391,32 +1448,66 @@ void BatchEngine::run() {
         for (int w = 0; w < n_windows_; w++)
             if (st[w] == ST_CAPACITY || st[w] == ST_OOM) redo.push_back(w);
         if (redo.empty()) break;
-        stats.retried += (int32_t)redo.size();
-        launch(redo.data(), (int32_t)redo.size(), attempt);
+        if (attempt == 1) stats.fallback = (int32_t)redo.size();
+        else stats.retried += (int32_t)redo.size();
+        launch(redo.data(), (int32_t)redo.size(), default_caps(attempt));
     }
 }
 
-void BatchEngine::launch(const int32_t* windows, int32_t count, int scale) {
+int BatchEngine::ring_blocks() const {
+    const int m = max_len_ + 1;
+    const int wb = p_.b + (p_.f ? m / p_.f : 0);
+    // adaptive rows can grow to the full query width: their ring rows are full width
+    int rb = p_.f > 0 && !p_.ab_band ? std::min(m / BLK + 2, (2 * wb) / BLK + 4) : m / BLK + 2;
+    return std::max(rb, 4);
+}
+
+BatchEngine::Caps BatchEngine::default_caps(int scale) const {
+    // capacities estimated from the read lengths, scaled on retries
+    const bool adaptive = p_.f > 0 && p_.ab_band;
+    const int m = max_len_ + 1;
+    const int wb = p_.b + (p_.f ? m / p_.f : 0);
+    const int64_t est = 2 + (int64_t)max_len_ + (int64_t)(0.2 * (double)max_win_bases_) + 256;
+    const int64_t NC64 = std::min<int64_t>(std::min<int64_t>(2 + max_win_bases_, est * scale), 60000);
+    Caps c;
+    c.NC = (int32_t)std::max<int64_t>(NC64, 64);
+    const int rb = ring_blocks();
+    const int tb_blocks = adaptive ? std::min(m / BLK + 2, (std::min(m / BLK + 2, (4 * wb) / BLK + 4)) * scale) : rb;
+    c.tb_cap = (int64_t)c.NC * tb_blocks * BLK * 2 * std::min(scale, 2) + 4096;
+    const int64_t spill_rows = std::min<int64_t>(c.NC, std::max<int64_t>(c.NC / (adaptive ? 8 : 4), 64) * scale);
+    c.spill = spill_rows * rb * 16;
+    return c;
+}
+
+void BatchEngine::set_plan(const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill, const float* cost) {
+    if (!nodes) {
+        plan_nodes_.clear();
+        plan_tb_.clear();
+        plan_spill_.clear();
+        plan_order_.clear();
+        return;
+    }
+    plan_nodes_.assign(nodes, nodes + n_windows_);
+    plan_tb_.assign(tb_bytes, tb_bytes + n_windows_);
+    plan_spill_.assign(spill, spill + n_windows_);
+    plan_order_.resize(n_windows_);
+    std::iota(plan_order_.begin(), plan_order_.end(), 0);
+    std::stable_sort(plan_order_.begin(), plan_order_.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+}
+
+void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps) {
     cudaStream_t s = (cudaStream_t)stream_;
     int sms = 0;
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attr");
     const bool adaptive = p_.f > 0 && p_.ab_band;
-    // capacities from the data, scaled on retries
-    const int64_t est = 2 + (int64_t)max_len_ + (int64_t)(0.2 * (double)max_win_bases_) + 256;
-    const int64_t NC64 = std::min<int64_t>(std::min<int64_t>(2 + max_win_bases_, est * scale), 60000);
-    const int32_t NC = (int32_t)std::max<int64_t>(NC64, 64);
+    const int32_t NC = std::max(caps.NC, 64);
     const int32_t EC = 3 * NC;
     const int32_t QC = max_len_ + 8;
-    const int m = max_len_ + 1;
-    const int wb = p_.b + (p_.f ? m / p_.f : 0);
-    int ring_blocks = p_.f > 0 ? std::min(m / BLK + 2, (2 * wb) / BLK + 4) : m / BLK + 2;
-    if (adaptive) ring_blocks = std::min(m / BLK + 2, (4 * wb) / BLK + 4);
-    ring_blocks = std::max(ring_blocks, 4);
-    const int tb_blocks = adaptive ? std::min(m / BLK + 2, ring_blocks * scale) : ring_blocks;
+    const int ring_blocks = this->ring_blocks();
     const int32_t ring_rows = 32;
-    const int64_t spill_rows = std::min<int64_t>(NC, std::max<int64_t>(NC / 4, 64) * scale);
-    const int64_t tb_cap = (int64_t)NC * tb_blocks * BLK * 2 * std::min(scale, 2) + 4096;
-    SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill_rows, tb_cap, adaptive);
+    const int64_t tb_cap = (caps.tb_cap + 4095) / 4096 * 4096;
+    const int64_t spill = (caps.spill + 63) / 64 * 64;
+    SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill, tb_cap, adaptive);
     const int warps = warps_per_block;
     const int smem_w = smem_per_warp;
     const size_t dyn = (size_t)warps * smem_w;
@@ -1469,11 +1560,7 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, int scale) {
 
     char* d = (char*)d_in_;
     char* o = (char*)d_out_;
-    if (windows != order_.data() || count != n_windows_)
-        cuda_check(cudaMemcpyAsync(d + off_order_, windows, 4 * (size_t)count, cudaMemcpyHostToDevice, s), "H2D order");
-    else
-        cuda_check(cudaMemcpyAsync(d + off_order_, order_.data(), 4 * (size_t)count, cudaMemcpyHostToDevice, s),
-                   "H2D order");
+    cuda_check(cudaMemcpyAsync(d + off_order_, windows, 4 * (size_t)count, cudaMemcpyHostToDevice, s), "H2D order");
     BatchArgs A;
     A.seq = (const uint8_t*)(d + off_seq_);
     A.read_off = (const int64_t*)(d + off_roff_);
@@ -1497,6 +1584,7 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, int scale) {
     A.status = (int32_t*)(o + out_status_);
     A.cells = (int64_t*)(o + out_cells_);
     A.phase = (int64_t*)(o + out_phase_);
+    A.rstats = (int32_t*)(o + out_rstats_);
     cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
     cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
     if (stat) {
@@ -1553,6 +1641,19 @@ void BatchEngine::download(std::vector<std::string>& cons, std::vector<int32_t>&
         stats.cells += cl[w];
         stats.failed += st[w] != ST_OK;
     }
+}
+
+}  // namespace pb
+
+namespace pb {
+
+void BatchEngine::read_stats(std::vector<int32_t>& out) {
+    cudaStream_t s = (cudaStream_t)stream_;
+    out.resize((size_t)NRSTAT * n_reads_);
+    if (n_reads_ == 0) return;
+    cuda_check(cudaMemcpyAsync(out.data(), (char*)d_out_ + out_rstats_, 4 * (size_t)NRSTAT * n_reads_,
+                               cudaMemcpyDeviceToHost, s), "D2H read stats");
+    cuda_check(cudaStreamSynchronize(s), "D2H read stats");
 }
 
 }  // namespace pb

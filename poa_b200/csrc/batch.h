@@ -24,6 +24,8 @@ struct BatchInput {
     int32_t n_windows;
 };
 
+constexpr int NRSTAT = 8;
+
 struct BatchStats {
     double kernel_ms = 0.0;   // device time of the last run() (CUDA events)
     int64_t cells = 0;        // DP band cells of the last run
@@ -33,6 +35,7 @@ struct BatchStats {
     int64_t h2d_bytes = 0, d2h_bytes = 0;
     int32_t failed = 0;       // windows that ended with a non-OK status
     int32_t retried = 0;      // windows re-run with larger capacities
+    int32_t fallback = 0;     // windows that outgrew the plan's sizing (re-run with the default sizing)
     int32_t launches = 0;     // kernel launches of the last run()
     // summed lane-0 clock cycles per phase over all windows: view build, DP
     // fill, backtrack, fusion, topological sort, consensus
@@ -49,8 +52,22 @@ class BatchEngine {
     void run();
     // Per-window consensus (ASCII) and status of the last run().
     void download(std::vector<std::string>& cons, std::vector<int32_t>& status);
+    // Resource plan of the uploaded windows (a band proposer's prediction), one
+    // value per window: graph nodes, traceback record bytes and spilled
+    // row-store entries of its largest alignment, and a relative cost (the
+    // windows run largest first). The plan sizes the slots only; every DP
+    // still runs the reference's band, and a window that outgrows its slot is
+    // re-run with the default sizing (counted in stats.fallback). nullptr
+    // clears the plan. Cleared by upload().
+    void set_plan(const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill, const float* cost);
     // Device-side totals only (no consensus copy): cells and failures.
     void sync_stats();
+    // Per read of the last run(), NRSTAT values: [0] widest DP row in blocks,
+    // [1] band cells, [2] DP rows, [3] graph nodes after fusing the read,
+    // [4] traceback record bytes, [5] spilled row-store entries (int32),
+    // [6] graph edges after fusing the read, [7] zero. A window's first read
+    // has no DP ([0..2], [4], [5] zero).
+    void read_stats(std::vector<int32_t>& out);
     BatchStats stats;
     int32_t warps_per_block = 4;
     int32_t blocks_per_sm = 3;  // 3: 168-register build; >= 4: 128-register build (occupancy still caps it)
@@ -59,8 +76,17 @@ class BatchEngine {
 
   private:
     void ensure(void** ptr, size_t* cap, size_t bytes);
-    // one persistent launch over `count` windows (ids), capacities scaled by `scale`
-    void launch(const int32_t* windows, int32_t count, int scale);
+    struct Caps {
+        int32_t NC;      // graph nodes per slot
+        int64_t tb_cap;  // traceback record bytes
+        int64_t spill;   // spilled row-store entries (int32)
+    };
+    Caps default_caps(int scale) const;
+    int ring_blocks() const;
+    // one persistent launch over `count` windows (ids) with slots of the given capacities
+    void launch(const int32_t* windows, int32_t count, const Caps& caps);
+    std::vector<int32_t> plan_nodes_, plan_order_;
+    std::vector<int64_t> plan_tb_, plan_spill_;
     int device_;
     void* stream_ = nullptr;
     void* ev0_ = nullptr;
@@ -74,7 +100,7 @@ class BatchEngine {
     void* d_slots_ = nullptr;   size_t d_slots_cap_ = 0;
     void* h_out_ = nullptr;     size_t h_out_cap_ = 0;   // pinned mirror of d_out_
     size_t off_seq_ = 0, off_roff_ = 0, off_rlen_ = 0, off_woff_ = 0, off_order_ = 0, off_ctr_ = 0;
-    size_t out_cons_ = 0, out_len_ = 0, out_status_ = 0, out_cells_ = 0, out_phase_ = 0, out_bytes_ = 0;
+    size_t out_cons_ = 0, out_len_ = 0, out_status_ = 0, out_cells_ = 0, out_phase_ = 0, out_rstats_ = 0, out_bytes_ = 0;
     std::vector<int32_t> order_;
 };
 

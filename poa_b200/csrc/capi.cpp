@@ -309,6 +309,16 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
     for (int k = 0; k < 6; k++) o[6 + k] = s.phase_cycles[k];
     o[12] = s.launches;
     o[13] = s.retried;
+    o[14] = s.fallback;
+    o[15] = (int64_t)(s.kernel_ms * 1000.0);
+    return POA_OK;
+}
+
+int poa_batch_plan(poa_ctx* ctx, const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill,
+                   const float* cost) {
+    if (!ctx || !ctx->batch) return fail(ctx, POA_BAD_ARG, "no uploaded batch");
+    if (nodes && (!tb_bytes || !spill || !cost)) return fail(ctx, POA_BAD_ARG, "incomplete plan");
+    ctx->batch->set_plan(nodes, tb_bytes, spill, cost);
     return POA_OK;
 }
 
@@ -336,6 +346,19 @@ void* poa_alloc_pinned(size_t bytes) {
 
 void poa_free_pinned(void* ptr) {
     if (ptr) cudaFreeHost(ptr);
+}
+
+int poa_batch_read_stats(poa_ctx* ctx, int32_t* out, int64_t cap) {
+    if (!ctx || !ctx->batch || !out) return fail(ctx, POA_BAD_ARG, "null argument");
+    try {
+        std::vector<int32_t> v;
+        ctx->batch->read_stats(v);
+        if ((int64_t)v.size() > cap) return fail(ctx, POA_BAD_ARG, "read stats buffer too small");
+        std::memcpy(out, v.data(), 4 * v.size());
+        return POA_OK;
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
 }
 
 int poa_stats(const poa_ctx* ctx, int64_t* o) {

@@ -1,21 +1,30 @@
-"""Benchmark: batched POA polishing windows on B200.
+"""Benchmark: batched POA windows on B200, with the learned band proposer.
 
-Workload (one step): 20,000 independent polishing windows (template
-500 +- 100 bp, 4-64 reads, 8 % error split 4:3:3 into substitutions,
-insertions and deletions; seeded synthetic data), each aligned progressively
-into its own POA graph in minipoa's default consensus mode (static band
-b=100, f=40, scoring 2/-4/-4/-2); output one consensus per window,
-bit-exact with minipoa.
+Default workload (one step): 5,000 independent learned-band windows (template
+2,000 bp, 20-100 reads, 15 % error split 4:3:3 into substitutions, insertions
+and deletions, 1 % chimeric reads; seeded synthetic data), each aligned
+progressively into its own POA graph with minipoa's adaptive band (-B,
+scoring 2/-4/-4/-2, b=100 f=40); output one consensus per window, bit-exact
+with minipoa. The learned band proposer plans every window's device slot
+inside the timed step (features, network, plan, then the persistent batch
+kernel; windows that outgrow their slot are re-run and counted as fallback).
+``--workload polishing``: 20,000 polishing windows (500 +- 100 bp, 4-64
+reads, 8 % error, static band), no proposer.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload learned_band|polishing]
 
 value  windows/s over all ranks with the inputs resident in HBM (device time
-       of the persistent batch kernel, CUDA events on its stream).
+       of the whole step: proposer plan + batch kernel + re-runs, CUDA events
+       on the engine's stream).
 e2e    windows/s through the public C ABI (poa_batch_consensus) with the
-       inputs in pinned host memory: upload, kernel, consensus download.
-Multi-GPU: every rank runs its own 20,000 windows (weak scaling, no
-collective on the data path; torch.distributed only for the barrier and the
-max over ranks of the time).
+       inputs in pinned host memory: upload, plan, kernel, consensus download.
+plain_kernel  windows/s of the plain single-alignment kernel path (poa_run:
+       one CTA per poa() call, graph fused on the host) on a sample of the
+       same windows, and the batched engine's speed-up over it.
+Multi-GPU: every rank runs its own windows (weak scaling, no collective on
+the data path; torch.distributed only for the barrier and the max over ranks
+of the time).
 ``--impl reference`` times the reference's own CPU build (oracle/_ref/minipoa,
 compiled from the reference sources) on a bounded sample of the same
 windows with every host core, one process per window.
@@ -38,23 +47,36 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "windows/s & GCUPS on 1 B200: learned-band+batched vs plain kernel, bit-exact"
-WORKLOAD = "polishing_windows: 20000 windows, template 500+-100 bp, 4-64 reads, 8% error (4:3:3), consensus"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "minipoa")
 PORT_BIN = os.path.join(ROOT, "oracle", "build", "poa_oracle")
 # algorithmic work per DP cell: 1 byte of traceback record written
-# (SURVEY-style unit: cell = one computed band cell, (Be-Bs-1)*8 per row)
+# (cell = one computed band cell, (Be-Bs-1)*8 per row)
 BYTES_PER_CELL = 1.0
 # int32 operations per cell and per edge-cell of the recurrence
 OPS_PER_CELL, OPS_PER_EDGE_CELL = 5, 7
+
+WORKLOADS = {
+    "learned_band": {
+        "gen": "learned_band_windows", "seed": 5, "windows": 5000, "opts": ["-B"], "proposer": True,
+        "steps": 1, "ref_windows_per_core": 1,
+        "desc": "learned_band_windows: 5000 windows, template 2000 bp, 20-100 reads, 15% error (4:3:3), "
+                "1% chimeric reads; adaptive band -B; consensus",
+        "mode": "consensus, adaptive band (-B) b=100 f=40, learned band proposer sizes the slots"},
+    "polishing": {
+        "gen": "polishing_windows", "seed": 4, "windows": 20000, "opts": [], "proposer": False,
+        "steps": 5, "ref_windows_per_core": 40,
+        "desc": "polishing_windows: 20000 windows, template 500+-100 bp, 4-64 reads, 8% error (4:3:3), consensus",
+        "mode": "consensus, static band b=100 f=40"},
+}
 
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def shard_seed(rank: int) -> int:
-    """Seed of rank r's windows: every rank runs its own 20,000 windows (weak scaling)."""
-    return 4 + 1000 * rank
+def shard_seed(rank: int, base: int = 5) -> int:
+    """Seed of rank r's windows: every rank runs its own windows (weak scaling)."""
+    return base + 1000 * rank
 
 
 def whole_job_rate(world: int, units_per_rank: int, steps: int, t_max: float) -> float:
@@ -175,9 +197,10 @@ def load_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "src": "fallback", "sm_max_mhz": 1965.0}
 
 
-def profile_traffic_per_cell():
-    """DRAM bytes per DP cell of k_batch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_batch_dram.json")
+def profile_traffic_per_cell(workload: str):
+    """DRAM bytes per DP cell of k_batch from the committed ncu summary of the workload."""
+    name = {"polishing": "k_batch_dram.json", "learned_band": "k_batch_dram_learned_band.json"}[workload]
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     with open(p) as fh:
@@ -201,41 +224,53 @@ def write_windows(ws, idx, d):
     return paths
 
 
-def run_cpu_windows(binary, paths, cores):
+def run_cpu_windows(binary, paths, cores, opts=()):
     def one(fa):
-        return subprocess.run([binary, fa], capture_output=True, check=True).stdout
+        return subprocess.run([binary, fa] + list(opts), capture_output=True, check=True).stdout
     with ThreadPoolExecutor(max_workers=cores) as ex:
         return list(ex.map(one, paths))
 
 
-def cpu_sample(ws, seconds, cores, binary):
+def cpu_sample(ws, seconds, cores, binary, opts=(), chunk_per_core=4):
     """Windows/s of the CPU binary over windows 0, 1, ... of ws: chunks of
-    4 windows per core until about `seconds` of wall time have passed."""
+    `chunk_per_core` windows per core until about `seconds` of wall time."""
     outs = []
     n = 0
     with tempfile.TemporaryDirectory() as d:
         t0 = time.perf_counter()
         while n < ws.n_windows and time.perf_counter() - t0 < seconds:
-            idx = range(n, min(ws.n_windows, n + 4 * cores))
-            outs.extend(run_cpu_windows(binary, write_windows(ws, idx, d), cores))
+            idx = range(n, min(ws.n_windows, n + chunk_per_core * cores))
+            outs.extend(run_cpu_windows(binary, write_windows(ws, idx, d), cores, opts))
             n = idx.stop
         dt = time.perf_counter() - t0
     return n / dt, n, dt, outs
+
+
+def make_windows(wl, rank, n):
+    from poa_b200 import synth
+    return getattr(synth, wl["gen"])(seed=shard_seed(rank, wl["seed"]), n_windows=n)
 
 
 # --------------------------------------------------------------------- arms
 def ours(args, world, rank, local, D):
     import poa_b200
     from poa_b200 import synth
+    wl = WORKLOADS[args.workload]
+    nwin = args.windows or wl["windows"]
     t0 = time.perf_counter()
-    ws = synth.polishing_windows(seed=shard_seed(rank), n_windows=args.windows)
+    ws = make_windows(wl, rank, nwin)
     log(f"[rank {rank}] generated {ws.n_windows} windows / {ws.n_reads} reads in {time.perf_counter() - t0:.1f}s")
     try:
         import torch
         torch.cuda.set_device(local)
     except Exception:
         pass
-    ctx = poa_b200.Context(poa_b200.Params(), device=local)
+    params = poa_b200.Params.from_cli(wl["opts"])
+    ctx = poa_b200.Context(params, device=local)
+    prop = None
+    if wl["proposer"] and not args.no_proposer:
+        prop = poa_b200.Proposer(device=local, weights=poa_b200.PROP_WEIGHTS)
+        ctx.batch_use_proposer(prop)
     if args.max_blocks:
         ctx.batch_config(max_blocks=args.max_blocks)
     if args.blocks_per_sm:
@@ -243,17 +278,22 @@ def ours(args, world, rank, local, D):
     if args.smem_per_warp:
         ctx.batch_config(smem_per_warp=args.smem_per_warp)
 
-    # ---- device-resident leg
+    # ---- device-resident leg: plan + kernel(s) per step, device-timed
     ctx.batch_upload(ws)
-    for _ in range(args.warmup):
-        ctx.batch_run()
+    for k in range(args.warmup):
+        ms = ctx.batch_run()
+        log(f"[rank {rank}] warm-up {k}: {ms / 1e3:.2f}s")
     D.barrier()
     clk = ClockSampler(gpu_uuid(local))
-    dev_ms = []
-    launches = 0
+    dev_ms, kern_ms, plan_ms = [], [], []
+    launches = fallback = 0
     for _ in range(args.steps):
         dev_ms.append(ctx.batch_run())
-        launches += ctx.batch_stats()["launches"]
+        st = ctx.batch_stats()
+        kern_ms.append(st["kernel_us"] / 1e3)
+        plan_ms.append(st["plan_us"] / 1e3)
+        launches += st["launches"]
+        fallback += st["fallback"]
     D.barrier()
     clocks = clk.stop()
     st = ctx.batch_stats()
@@ -261,6 +301,11 @@ def ours(args, world, rank, local, D):
     cells = st["cells"]
     failed = int(D.sum(st["failed"]))
     cons, status = ctx.batch_download()
+    # proposer kernels per step: features, 3 im2col + 5 GEMM + pool + de-standardise
+    # per 4096-read chunk, conversion, plan
+    if prop is not None:
+        chunks = -(-ws.n_reads // 4096)
+        launches += args.steps * (2 + chunks * 11)
 
     # ---- end-to-end leg through the C ABI with pinned host buffers
     e2e = None
@@ -272,7 +317,8 @@ def ours(args, world, rank, local, D):
             holders.append(h)
             arrs.append(v)
         pws = synth.WindowSet(seq=arrs[0], read_off=arrs[1], read_len=arrs[2], win_off=arrs[3])
-        for _ in range(max(1, args.warmup)):
+        e2e_warm = args.e2e_warmup if args.e2e_warmup >= 0 else (1 if wl["steps"] > 1 else 0)
+        for _ in range(e2e_warm):
             ctx.batch_consensus(pws)
         D.barrier()
         t0 = time.perf_counter()
@@ -283,28 +329,36 @@ def ours(args, world, rank, local, D):
         st2 = ctx.batch_stats()
         e2e = {"value": whole_job_rate(world, ws.n_windows, args.steps, t_e2e), "unit": "windows/s",
                "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
-               "ms_per_step": 1e3 * t_e2e / args.steps, "api": "poa_batch_consensus"}
+               "ms_per_step": 1e3 * t_e2e / args.steps, "api": "poa_batch_consensus", "warmup": e2e_warm,
+               "note": "host wall clock around upload + plan + kernel + download"
+                       + ("; the same context ran the device leg's warm-up steps first" if not e2e_warm else "")}
         assert c2 == cons and s2 == status, "end-to-end run disagrees with the device-resident run"
         for h in holders:
             h.close()
 
     value = whole_job_rate(world, ws.n_windows, args.steps, t_dev)
-    kernel_s = t_dev / args.steps
+    kernel_s = D.max(sum(kern_ms) / 1e3) / args.steps
     peaks = load_peaks()
     achieved = cells * BYTES_PER_CELL / kernel_s / 1e9
-    tpc = profile_traffic_per_cell()
+    tpc = profile_traffic_per_cell(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_src": peaks["src"],
                 "traffic": (tpc * cells if tpc is not None else None),
-                "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL, "kernel": "k_batch"}
+                "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL, "kernel": "k_batch",
+                "kernel_s_per_step": kernel_s,
+                "int_ops_frac": (cells * OPS_PER_CELL / kernel_s) / int_peak_ops(clocks.get("sm_mhz")),
+                "int_ops_note": "lower bound: 5 int32 ops per cell (edge-cell ops not counted), "
+                                "nominal peak 148 SMs x 128 lanes x median SM clock"}
     line = {
         "metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * kernel_s, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": WORKLOAD, "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
-                   "bases_per_rank": int(ws.seq.shape[0]), "mode": "consensus, static band b=100 f=40",
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded; no dataset)",
+        "config": {"workload": wl["desc"], "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
+                   "bases_per_rank": int(ws.seq.shape[0]), "mode": wl["mode"] if prop else
+                   wl["mode"].replace(", learned band proposer sizes the slots", ""),
                    "parallelism": f"windows sharded over {world} GPU(s)",
-                   "l2": "inputs (%.0f MB) larger than L2 (126 MB)" % (ws.seq.shape[0] / 1e6)},
+                   "l2": "inputs (%.0f MB) and slots (%.1f GB) larger than L2 (126 MB)"
+                         % (ws.seq.shape[0] / 1e6, st["slots"] * st["slot_bytes"] / 1e9)},
         "gcups": world * cells * args.steps / t_dev / 1e9,
         "cells_per_step": cells, "failed_windows": failed,
         "gpu_launches": launches, "retried_windows": st["retried"], "e2e": e2e, "roofline": roofline, "clocks": clocks,
@@ -312,65 +366,90 @@ def ours(args, world, rank, local, D):
         "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
         "phase_mcycles_per_window": {k: v / 1e6 / ws.n_windows for k, v in st["phase_cycles"].items()},
     }
+    if prop is not None:
+        line["proposer"] = {"fallback_windows": int(D.sum(fallback)),
+                            "fallback_rate": D.sum(fallback) / (world * ws.n_windows * args.steps),
+                            "plan_ms_per_step": sum(plan_ms) / args.steps,
+                            "weights": os.path.relpath(poa_b200.PROP_WEIGHTS, ROOT),
+                            "exact": "the plan sizes slots only; every DP runs the reference band"}
+    if rank == 0 and world == 1 and args.plain_windows > 0:
+        # the plain single-alignment kernel on the first windows of the same set
+        n = min(args.plain_windows, ws.n_windows)
+        t0 = time.perf_counter()
+        same = 0
+        for w in range(n):
+            txt, _ = ctx.run(ws.window_reads(w))
+            same += txt == b">consensus sequence\n" + cons[w] + b"\n"
+        dt = time.perf_counter() - t0
+        line["plain_kernel"] = {"value": n / dt, "unit": "windows/s", "windows": n, "identical_consensus": same,
+                                "path": "poa_run: one CTA per poa() call (k_plain), graph fused on the host",
+                                "speedup": value / (n / dt)}
     if rank == 0 and world == 1 and not args.no_cpu:
         binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
         kind = "reference" if binary == REF_BIN else "port"
         cores = len(os.sched_getaffinity(0))
-        v, n, dt, outs = cpu_sample(ws, args.cpu_seconds, cores, binary)
+        v, n, dt, outs = cpu_sample(ws, args.cpu_seconds, cores, binary, wl["opts"],
+                                    chunk_per_core=1 if wl["proposer"] else 4)
         same = sum(1 for w in range(n) if outs[w] == b">consensus sequence\n" + cons[w] + b"\n")
         line["cpu_baseline"] = {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
-                                "sample": f"first {n} of the {ws.n_windows} windows, one process per window, "
-                                          f"{dt:.1f}s wall"}
+                                "sample": f"first {n} of the {ws.n_windows} windows, one process per window "
+                                          f"({' '.join(wl['opts']) or 'default options'}), {dt:.1f}s wall"}
         line["parity_sample"] = {"windows": n, "identical_consensus": same}
     ctx.close()
     return line
 
 
 def reference(args, world, rank, local, D):
-    from poa_b200 import synth
     if rank != 0:
         return None
+    wl = WORKLOADS[args.workload]
     binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
     kind = "reference" if binary == REF_BIN else "port"
     cores = len(os.sched_getaffinity(0))
-    ws = synth.polishing_windows(seed=4, n_windows=min(args.windows, args.ref_windows_per_step * cores))
-    per_step = min(ws.n_windows, args.ref_windows_per_step * cores)
+    per_step = min(args.windows or wl["windows"], wl["ref_windows_per_core"] * cores)
+    ws = make_windows(wl, 0, per_step)
     with tempfile.TemporaryDirectory() as d:
         paths = write_windows(ws, range(per_step), d)
         for _ in range(args.warmup):
-            run_cpu_windows(binary, paths[:cores], cores)
+            run_cpu_windows(binary, paths[:cores], cores, wl["opts"])
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            run_cpu_windows(binary, paths, cores)
+            run_cpu_windows(binary, paths, cores, wl["opts"])
         dt = time.perf_counter() - t0
     v = per_step * args.steps / dt
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "windows/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": WORKLOAD, "windows_per_step": per_step},
+            "config": {"workload": wl["desc"], "windows_per_step": per_step, "mode": wl["mode"]},
             "cpu_baseline": {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
-                             "sample": f"{per_step} windows per step, one {kind} process per window, "
-                                       f"{cores} concurrent"},
+                             "sample": f"{per_step} windows per step, one {kind} process per window "
+                                       f"({' '.join(wl['opts']) or 'default options'}), {cores} concurrent"},
             "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default: 1 learned_band, 5 polishing)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--windows", type=int, default=20000)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--ref-windows-per-step", type=int, default=40)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="learned_band")
+    ap.add_argument("--windows", type=int, default=0, help="windows per rank (default: the workload's)")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--plain-windows", type=int, default=2,
+                    help="windows timed on the plain single-alignment kernel path (0 = skip)")
+    ap.add_argument("--e2e-warmup", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-proposer", action="store_true", help="learned_band without the proposer's plan")
     ap.add_argument("--max-blocks", type=int, default=0,
                     help="cap the persistent grid (small profiling captures); 0 = one full wave")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="batch kernel variant: 3 (default) or 4")
-    ap.add_argument("--smem-per-warp", type=int, default=0, help="shared memory per warp in bytes (default 16384)")
+    ap.add_argument("--smem-per-warp", type=int, default=0, help="shared memory per warp in bytes")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = WORKLOADS[args.workload]["steps"]
     world, rank, local = dist_env()
     if args.impl == "reference":
         if rank != 0:

@@ -135,9 +135,11 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * backtrack, graph fusion, topological sort and consensus phases,
  * [12] kernel launches of the last run, [13] windows re-run with larger
  * capacities, [14] windows that outgrew the plan's sizing (poa_batch_plan)
- * and were re-run with the default sizing, [15] device time of the last run
- * in microseconds. */
-int poa_batch_stats(poa_ctx* ctx, int64_t* out16);
+ * and were re-run with the default sizing, [15] device time of the batch
+ * kernel launches of the last run in microseconds, [16] device time of the
+ * whole last run (plan, launches, re-runs) in microseconds, [17] device time
+ * of the proposer's plan in microseconds (0 without a proposer). */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out18);
 /* Resource plan for the uploaded windows (no counterpart in the reference:
  * the reference allocates per alignment). One value per window: graph nodes,
  * traceback record bytes and spilled row-store entries (int32) of its
@@ -224,6 +226,46 @@ void poa_free_pinned(void* ptr);
  * [5] D2H bytes. */
 int poa_stats(const poa_ctx* ctx, int64_t* out6);
 int poa_set_timing(poa_ctx* ctx, int on);
+
+/* ---- learned band proposer (no counterpart in the reference) -----------
+ *
+ * minipoa allocates each alignment's DP matrices when it runs it
+ * (src/align.cpp:1397). The batch engine instead sizes every window's
+ * device slot before one persistent launch. The proposer predicts the sizes
+ * from minimizer features (k=15, w=10) of each window's reads: a 3-layer
+ * 1D convolution (64 channels) plus MLP, BF16 weights, FP32 accumulation,
+ * trained on the band statistics of plain runs (poa_batch_read_stats). The
+ * plan never changes a band: results are identical with or without it. */
+typedef struct poa_proposer poa_proposer;
+/* Number of floats in a weight vector: the network parameters, then output
+ * mean[4], output std[4], node margin, record-byte margin, spilled
+ * row-store entries per row, minimum spill entries. */
+int poa_prop_nweights(void);
+/* NULL on failure (no CUDA device or no memory). Starts from a fixed random
+ * initialisation. */
+poa_proposer* poa_prop_create(int device);
+void poa_prop_destroy(poa_proposer* p);
+const char* poa_prop_last_error(const poa_proposer* p);
+int poa_prop_set_weights(poa_proposer* p, const float* w);
+int poa_prop_get_weights(poa_proposer* p, float* w);
+/* Train on X [n][32 bins][8 channels] (poa_batch_features) against raw
+ * targets Y [n][4] per read: new graph nodes per query base, band cells /
+ * (DP rows * (qlen + 1)), record bytes per cell, mean band centre / (qlen + 1).
+ * Mini-batch Adam on the GPU; per-epoch mean losses to `losses` (may be NULL).
+ * The output standardisation is taken from Y; margins stay as set. */
+int poa_prop_train(poa_proposer* p, const float* X, const float* Y, int64_t n, int32_t epochs, int32_t batch,
+                   float lr, uint64_t seed, float* losses);
+/* Raw predictions Y [n][4] for features X [n][32][8]. */
+int poa_prop_predict(poa_proposer* p, const float* X, int64_t n, float* Y);
+/* Features of every read of the uploaded batch: n_reads * 32 * 8 floats. */
+int poa_batch_features(poa_ctx* ctx, poa_proposer* p, float* X, int64_t cap);
+/* Features, prediction and per-window plan on the device, then
+ * poa_batch_plan with it: the next poa_batch_run uses the planned slots. */
+int poa_batch_propose(poa_ctx* ctx, poa_proposer* p);
+/* Let every following poa_batch_run (and poa_batch_consensus) plan its
+ * windows with `p` first, inside the timed run; NULL turns it off. The
+ * proposer must outlive its use. */
+int poa_batch_use_proposer(poa_ctx* ctx, poa_proposer* p);
 
 #ifdef __cplusplus
 }

@@ -119,6 +119,19 @@ def lib() -> ctypes.CDLL:
     L.poa_batch_config.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
     L.poa_batch_read_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
     L.poa_batch_plan.argtypes = [ctypes.c_void_p] * 5
+    L.poa_prop_create.restype = ctypes.c_void_p
+    L.poa_prop_create.argtypes = [ctypes.c_int]
+    L.poa_prop_destroy.argtypes = [ctypes.c_void_p]
+    L.poa_prop_last_error.restype = ctypes.c_char_p
+    L.poa_prop_last_error.argtypes = [ctypes.c_void_p]
+    L.poa_prop_set_weights.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.poa_prop_get_weights.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.poa_prop_train.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                 ctypes.c_int32, ctypes.c_float, ctypes.c_uint64, ctypes.c_void_p]
+    L.poa_prop_predict.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    L.poa_batch_features.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
+    L.poa_batch_propose.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.poa_batch_use_proposer.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.poa_alloc_pinned.restype = ctypes.c_void_p
     L.poa_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
@@ -240,6 +253,23 @@ class Context:
         self._check(lib().poa_batch_read_stats(self._h, out.ctypes.data, out.size))
         return out[:n]
 
+    def batch_features(self, prop: "Proposer"):
+        """float32 [n_reads, 32, 8] proposer features of the uploaded windows."""
+        import numpy as np
+        n = int(self._keep[2].shape[0]) if getattr(self, "_keep", None) is not None else 0
+        X = np.zeros((max(n, 1), PROP_BINS, PROP_CIN), dtype=np.float32)
+        self._check(lib().poa_batch_features(self._h, prop._h, X.ctypes.data, X.size))
+        return X[:n]
+
+    def batch_use_proposer(self, prop: Optional["Proposer"]) -> None:
+        """Plan every following batch run with ``prop`` (None: no proposer)."""
+        self._prop = prop  # keep it alive while the engine may use it
+        self._check(lib().poa_batch_use_proposer(self._h, prop._h if prop is not None else None))
+
+    def batch_propose(self, prop: "Proposer") -> None:
+        """Plan the uploaded windows' slots with the proposer (see poa_batch_propose)."""
+        self._check(lib().poa_batch_propose(self._h, prop._h))
+
     def batch_config(self, blocks_per_sm=None, max_blocks=None, smem_per_warp=None):
         """Launch shape of the batch kernel (see poa_batch_config)."""
         for key, val in ((0, blocks_per_sm), (1, max_blocks), (2, smem_per_warp)):
@@ -247,12 +277,12 @@ class Context:
                 self._check(lib().poa_batch_config(self._h, key, int(val)))
 
     def batch_stats(self) -> dict:
-        o = (ctypes.c_int64 * 16)()
+        o = (ctypes.c_int64 * 18)()
         self._check(lib().poa_batch_stats(self._h, o))
         names = ("view", "fill", "backtrack", "fusion", "topsort", "consensus")
         return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5],
                     phase_cycles={names[k]: o[6 + k] for k in range(6)}, launches=o[12], retried=o[13],
-                    fallback=o[14], kernel_us=o[15])
+                    fallback=o[14], kernel_us=o[15], run_us=o[16], plan_us=o[17])
 
     def batch_plan(self, nodes=None, tb_bytes=None, spill=None, cost=None):
         """Per-window resource plan (see poa_batch_plan); no arguments clears it."""
@@ -275,6 +305,77 @@ class Context:
         o = (ctypes.c_int64 * 6)()
         lib().poa_stats(self._h, o)
         return dict(launches=o[0], alignments=o[1], cells=o[2], kernel_us=o[3], h2d_bytes=o[4], d2h_bytes=o[5])
+
+
+PROP_BINS, PROP_CIN, PROP_OUT = 32, 8, 4
+PROP_WEIGHTS = os.path.join(_HERE, "proposer_weights.f32")
+
+
+class Proposer:
+    """The learned band proposer (poa_prop_* in include/poa_b200.h)."""
+
+    def __init__(self, device: int = 0, weights: Optional[str] = None):
+        self._h = lib().poa_prop_create(device)
+        if not self._h:
+            raise PoaError(8, "poa_prop_create failed (no CUDA device or out of memory)")
+        if weights is not None:
+            self.load(weights)
+
+    @staticmethod
+    def nweights() -> int:
+        return int(lib().poa_prop_nweights())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().poa_prop_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != 0:
+            raise PoaError(st, lib().poa_prop_last_error(self._h).decode(errors="replace"))
+
+    def get_weights(self):
+        import numpy as np
+        w = np.zeros(self.nweights(), dtype=np.float32)
+        self._check(lib().poa_prop_get_weights(self._h, w.ctypes.data))
+        return w
+
+    def set_weights(self, w) -> None:
+        import numpy as np
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        if w.shape != (self.nweights(),):
+            raise ValueError(f"expected {self.nweights()} weights, got {w.shape}")
+        self._check(lib().poa_prop_set_weights(self._h, w.ctypes.data))
+
+    def load(self, path: str = PROP_WEIGHTS) -> None:
+        import numpy as np
+        self.set_weights(np.fromfile(path, dtype="<f4"))
+
+    def save(self, path: str) -> None:
+        self.get_weights().astype("<f4").tofile(path)
+
+    def train(self, X, Y, epochs: int = 30, batch: int = 256, lr: float = 1e-3, seed: int = 1):
+        """Train on X [n,32,8] / raw targets Y [n,4]; returns the per-epoch losses."""
+        import numpy as np
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._check(lib().poa_prop_train(self._h, X.ctypes.data, Y.ctypes.data, X.shape[0], epochs, batch, lr, seed,
+                                         losses.ctypes.data))
+        return losses
+
+    def predict(self, X):
+        import numpy as np
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], PROP_OUT), dtype=np.float32)
+        self._check(lib().poa_prop_predict(self._h, X.ctypes.data, X.shape[0], Y.ctypes.data))
+        return Y
 
 
 class PinnedArray:

@@ -10,6 +10,7 @@
 // reference's sequential algorithms, run by lane 0; the window view of the
 // DP rows, the shifted query and the DP fill itself use the whole warp.
 #include "batch.h"
+#include "proposer.h"
 
 #include <cuda_runtime.h>
 
@@ -1148,6 +1149,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 g.hdr[0] = nn;
                 g.hdr[1] = ne;
                 g.hdr[2] = st;
+                A.rstats[(int64_t)r * NRSTAT + 3] = nn;
+                A.rstats[(int64_t)r * NRSTAT + 6] = ne;
             }
             __syncwarp();
             status = g.hdr[2];
@@ -1210,17 +1213,23 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         {
             // per-read band statistics
             int mbn = 0;
+            long long mid = 0;
             for (int i = lane; i < v.n; i += 32) {
                 const RowMeta rm = ((const RowMeta*)(s + L.meta))[i];
                 mbn = max(mbn, rm.Be - rm.Bs - 1);
+                mid += (long long)(rm.Bs + rm.Be - 1) * (BLK / 2);
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mbn = max(mbn, __shfl_xor_sync(0xffffffffu, mbn, o));
+            for (int o = 16; o > 0; o >>= 1) {
+                mbn = max(mbn, __shfl_xor_sync(0xffffffffu, mbn, o));
+                mid += __shfl_xor_sync(0xffffffffu, mid, o);
+            }
             if (lane == 0) {
                 int32_t* o = A.rstats + (int64_t)r * NRSTAT;
                 o[0] = mbn;
                 o[1] = a.out[3];
                 o[2] = v.n;
+                o[7] = v.n > 0 ? (int32_t)(mid * 1000 / ((long long)v.n * (len + 1))) : 0;
                 if constexpr (static_band) {
                     o[4] = a.out[4];  // record bytes and spilled row-store entries (view scan)
                     o[5] = a.out[5];
@@ -1319,11 +1328,13 @@ BatchEngine::BatchEngine(int device) : device_(device) {
     cudaStream_t s;
     cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
     stream_ = s;
-    cudaEvent_t e0, e1;
-    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
-    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
-    ev0_ = e0;
-    ev1_ = e1;
+    cudaEvent_t e[5];
+    for (int i = 0; i < 5; i++) cuda_check(cudaEventCreate(&e[i]), "cudaEventCreate");
+    ev0_ = e[0];
+    ev1_ = e[1];
+    evr0_ = e[2];
+    evr1_ = e[3];
+    evp_ = e[4];
 }
 
 BatchEngine::~BatchEngine() {
@@ -1332,8 +1343,8 @@ BatchEngine::~BatchEngine() {
     if (d_out_) cudaFree(d_out_);
     if (d_slots_) cudaFree(d_slots_);
     if (h_out_) cudaFreeHost(h_out_);
-    if (ev0_) cudaEventDestroy((cudaEvent_t)ev0_);
-    if (ev1_) cudaEventDestroy((cudaEvent_t)ev1_);
+    for (void* e : {ev0_, ev1_, evr0_, evr1_, evp_})
+        if (e) cudaEventDestroy((cudaEvent_t)e);
     if (stream_) cudaStreamDestroy((cudaStream_t)stream_);
 }
 
@@ -1411,10 +1422,21 @@ void BatchEngine::run() {
     stats.kernel_ms = 0.0;
     stats.retried = 0;
     stats.launches = 0;
-    if (n_reads_ > 0)
-        cuda_check(cudaMemsetAsync((char*)d_out_ + out_rstats_, 0, 4 * (size_t)NRSTAT * n_reads_, (cudaStream_t)stream_),
-                   "memset read stats");
     stats.fallback = 0;
+    stats.plan_ms = 0.0;
+    cudaStream_t rs = (cudaStream_t)stream_;
+    cuda_check(cudaEventRecord((cudaEvent_t)evr0_, rs), "event");
+    if (proposer_) {
+        std::vector<int32_t> nodes;
+        std::vector<int64_t> tb, spill;
+        std::vector<float> cost;
+        proposer_->plan(device_windows(), PROP_K, PROP_W, nodes, tb, spill, cost);
+        set_plan(nodes.data(), tb.data(), spill.data(), cost.data());
+        cuda_check(cudaEventRecord((cudaEvent_t)evp_, rs), "event");
+    }
+    if (n_reads_ > 0)
+        cuda_check(cudaMemsetAsync((char*)d_out_ + out_rstats_, 0, 4 * (size_t)NRSTAT * n_reads_, rs),
+                   "memset read stats");
     // With a plan, one pass sized by the plan's largest window, in the plan's
     // cost order; its windows that outgrow their slot fall back to the sizing
     // below. Without one, a first pass with capacities estimated from the read
@@ -1451,6 +1473,15 @@ void BatchEngine::run() {
         if (attempt == 1) stats.fallback = (int32_t)redo.size();
         else stats.retried += (int32_t)redo.size();
         launch(redo.data(), (int32_t)redo.size(), default_caps(attempt));
+    }
+    cuda_check(cudaEventRecord((cudaEvent_t)evr1_, rs), "event");
+    cuda_check(cudaEventSynchronize((cudaEvent_t)evr1_), "batch run");
+    float ms = 0.f;
+    cuda_check(cudaEventElapsedTime(&ms, (cudaEvent_t)evr0_, (cudaEvent_t)evr1_), "elapsed");
+    stats.run_ms = ms;
+    if (proposer_) {
+        cuda_check(cudaEventElapsedTime(&ms, (cudaEvent_t)evr0_, (cudaEvent_t)evp_), "elapsed");
+        stats.plan_ms = ms;
     }
 }
 
@@ -1646,6 +1677,21 @@ void BatchEngine::download(std::vector<std::string>& cons, std::vector<int32_t>&
 }  // namespace pb
 
 namespace pb {
+
+DeviceWindows BatchEngine::device_windows() const {
+    DeviceWindows d;
+    const char* b = (const char*)d_in_;
+    d.seq = (const uint8_t*)(b + off_seq_);
+    d.read_off = (const int64_t*)(b + off_roff_);
+    d.read_len = (const int32_t*)(b + off_rlen_);
+    d.win_off = (const int32_t*)(b + off_woff_);
+    d.n_reads = n_reads_;
+    d.n_windows = n_windows_;
+    d.max_len = max_len_;
+    d.max_win_bases = max_win_bases_;
+    d.stream = stream_;
+    return d;
+}
 
 void BatchEngine::read_stats(std::vector<int32_t>& out) {
     cudaStream_t s = (cudaStream_t)stream_;

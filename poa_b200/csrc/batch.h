@@ -26,8 +26,23 @@ struct BatchInput {
 
 constexpr int NRSTAT = 8;
 
+class Proposer;
+
+// Device copies of an uploaded batch (valid until the next upload).
+struct DeviceWindows {
+    const uint8_t* seq;
+    const int64_t* read_off;
+    const int32_t* read_len;
+    const int32_t* win_off;
+    int32_t n_reads, n_windows, max_len;
+    int64_t max_win_bases;
+    void* stream;
+};
+
 struct BatchStats {
-    double kernel_ms = 0.0;   // device time of the last run() (CUDA events)
+    double kernel_ms = 0.0;   // device time of the last run()'s kernel launches (CUDA events)
+    double run_ms = 0.0;      // device time of the whole last run(): plan, launches, re-runs
+    double plan_ms = 0.0;     // device time of the proposer's plan inside run()
     int64_t cells = 0;        // DP band cells of the last run
     int64_t dp_calls = 0;
     int32_t slots = 0;        // concurrent windows (warps) of the persistent launch
@@ -60,13 +75,17 @@ class BatchEngine {
     // re-run with the default sizing (counted in stats.fallback). nullptr
     // clears the plan. Cleared by upload().
     void set_plan(const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill, const float* cost);
+    DeviceWindows device_windows() const;
+    // Plan every run() with this proposer first (nullptr: no proposer).
+    void set_proposer(Proposer* p) { proposer_ = p; }
     // Device-side totals only (no consensus copy): cells and failures.
     void sync_stats();
     // Per read of the last run(), NRSTAT values: [0] widest DP row in blocks,
     // [1] band cells, [2] DP rows, [3] graph nodes after fusing the read,
     // [4] traceback record bytes, [5] spilled row-store entries (int32),
-    // [6] graph edges after fusing the read, [7] zero. A window's first read
-    // has no DP ([0..2], [4], [5] zero).
+    // [6] graph edges after fusing the read, [7] mean band centre (midpoint
+    // column over the DP rows) in thousandths of the query length. A window's
+    // first read has no DP ([0..2], [4], [5], [7] zero).
     void read_stats(std::vector<int32_t>& out);
     BatchStats stats;
     int32_t warps_per_block = 4;
@@ -85,6 +104,10 @@ class BatchEngine {
     int ring_blocks() const;
     // one persistent launch over `count` windows (ids) with slots of the given capacities
     void launch(const int32_t* windows, int32_t count, const Caps& caps);
+    Proposer* proposer_ = nullptr;
+    void* evr0_ = nullptr;
+    void* evr1_ = nullptr;
+    void* evp_ = nullptr;
     std::vector<int32_t> plan_nodes_, plan_order_;
     std::vector<int64_t> plan_tb_, plan_spill_;
     int device_;

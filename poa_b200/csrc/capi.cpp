@@ -11,6 +11,7 @@
 
 #include "batch.h"
 #include "gpu_engine.h"
+#include "proposer.h"
 
 struct poa_ctx {
     int device = 0;
@@ -20,7 +21,20 @@ struct poa_ctx {
     std::string err;
 };
 
+struct poa_proposer {
+    int device = 0;
+    pb::Proposer* prop = nullptr;
+    std::string err;
+};
+
 namespace {
+
+constexpr int kPropK = pb::PROP_K, kPropW = pb::PROP_W;
+
+int prop_fail(poa_proposer* p, int code, const std::string& msg) {
+    if (p) p->err = msg;
+    return code;
+}
 
 pb::Params to_params(const poa_params* c) {
     pb::Params p;
@@ -259,7 +273,7 @@ int poa_batch_run(poa_ctx* ctx, double* device_ms) {
     if (!ctx || !ctx->batch) return fail(ctx, POA_BAD_ARG, "nothing uploaded");
     try {
         ctx->batch->run();
-        if (device_ms) *device_ms = ctx->batch->stats.kernel_ms;
+        if (device_ms) *device_ms = ctx->batch->stats.run_ms;
         return POA_OK;
     } catch (const std::exception& e) {
         return fail(ctx, POA_CUDA, e.what());
@@ -311,6 +325,8 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
     o[13] = s.retried;
     o[14] = s.fallback;
     o[15] = (int64_t)(s.kernel_ms * 1000.0);
+    o[16] = (int64_t)(s.run_ms * 1000.0);
+    o[17] = (int64_t)(s.plan_ms * 1000.0);
     return POA_OK;
 }
 
@@ -372,6 +388,122 @@ int poa_stats(const poa_ctx* ctx, int64_t* o) {
 int poa_set_timing(poa_ctx* ctx, int on) {
     if (!ctx) return POA_BAD_ARG;
     ctx->eng->timing = on != 0;
+    return POA_OK;
+}
+
+
+/* ---- learned band proposer ---------------------------------------------- */
+
+int poa_prop_nweights(void) { return pb::PROP_NWEIGHTS; }
+
+poa_proposer* poa_prop_create(int device) {
+    poa_proposer* p = new poa_proposer();
+    p->device = device;
+    try {
+        p->prop = new pb::Proposer(device);
+    } catch (const std::exception&) {
+        delete p;
+        return nullptr;
+    }
+    return p;
+}
+
+void poa_prop_destroy(poa_proposer* p) {
+    if (!p) return;
+    delete p->prop;
+    delete p;
+}
+
+const char* poa_prop_last_error(const poa_proposer* p) { return p ? p->err.c_str() : "null proposer"; }
+
+int poa_prop_set_weights(poa_proposer* p, const float* w) {
+    if (!p || !w) return prop_fail(p, POA_BAD_ARG, "null argument");
+    try {
+        p->prop->set_weights(w);
+    } catch (const std::invalid_argument& e) {
+        return prop_fail(p, POA_BAD_ARG, e.what());
+    } catch (const std::exception& e) {
+        return prop_fail(p, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
+int poa_prop_get_weights(poa_proposer* p, float* w) {
+    if (!p || !w) return prop_fail(p, POA_BAD_ARG, "null argument");
+    try {
+        p->prop->get_weights(w);
+    } catch (const std::exception& e) {
+        return prop_fail(p, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
+int poa_prop_train(poa_proposer* p, const float* X, const float* Y, int64_t n, int32_t epochs, int32_t batch,
+                   float lr, uint64_t seed, float* losses) {
+    if (!p || !X || !Y) return prop_fail(p, POA_BAD_ARG, "null argument");
+    if (n <= 0 || epochs <= 0 || batch <= 0 || batch > 4096 || !(lr > 0.f))
+        return prop_fail(p, POA_BAD_ARG, "bad training arguments");
+    try {
+        p->prop->train(X, Y, n, epochs, batch, lr, seed, losses);
+    } catch (const std::exception& e) {
+        return prop_fail(p, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
+int poa_prop_predict(poa_proposer* p, const float* X, int64_t n, float* Y) {
+    if (!p || (n > 0 && (!X || !Y)) || n < 0) return prop_fail(p, POA_BAD_ARG, "bad argument");
+    if (n == 0) return POA_OK;
+    try {
+        p->prop->predict_host(X, n, Y);
+    } catch (const std::exception& e) {
+        return prop_fail(p, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
+int poa_batch_features(poa_ctx* ctx, poa_proposer* p, float* X, int64_t cap) {
+    if (!ctx || !ctx->batch || !p || !X) return fail(ctx, POA_BAD_ARG, "null argument or no uploaded batch");
+    try {
+        const pb::DeviceWindows dw = ctx->batch->device_windows();
+        const int64_t need = (int64_t)dw.n_reads * pb::PROP_BINS * pb::PROP_CIN;
+        if (need > cap) return fail(ctx, POA_BAD_ARG, "feature buffer too small");
+        if (need == 0) return POA_OK;
+        float* d = nullptr;
+        pb::cuda_check(cudaMalloc(&d, 4 * (size_t)need), "cudaMalloc(features)");
+        p->prop->features(dw, kPropK, kPropW, d, dw.stream);
+        const cudaError_t e1 = cudaMemcpyAsync(X, d, 4 * (size_t)need, cudaMemcpyDeviceToHost, (cudaStream_t)dw.stream);
+        const cudaError_t e2 = cudaStreamSynchronize((cudaStream_t)dw.stream);
+        cudaFree(d);
+        pb::cuda_check(e1 != cudaSuccess ? e1 : e2, "D2H features");
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
+int poa_batch_use_proposer(poa_ctx* ctx, poa_proposer* p) {
+    if (!ctx) return POA_BAD_ARG;
+    try {
+        if (!ctx->batch) ctx->batch = new pb::BatchEngine(ctx->device);
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
+    ctx->batch->set_proposer(p ? p->prop : nullptr);
+    return POA_OK;
+}
+
+int poa_batch_propose(poa_ctx* ctx, poa_proposer* p) {
+    if (!ctx || !ctx->batch || !p) return fail(ctx, POA_BAD_ARG, "null argument or no uploaded batch");
+    try {
+        std::vector<int32_t> nodes;
+        std::vector<int64_t> tb, spill;
+        std::vector<float> cost;
+        p->prop->plan(ctx->batch->device_windows(), kPropK, kPropW, nodes, tb, spill, cost);
+        ctx->batch->set_plan(nodes.data(), tb.data(), spill.data(), cost.data());
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_CUDA, e.what());
+    }
     return POA_OK;
 }
 

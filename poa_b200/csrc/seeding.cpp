@@ -17,24 +17,13 @@
 #include <cstring>
 
 #include "driver.h"
+#include "sketch.h"
 
 namespace pb {
 
 namespace {
 
 constexpr int32_t kInf = 1000000000;  // src/lchain.cpp:8
-
-// Thomas Wang's 64-bit integer hash as used by the sketch (src/minimizer.cpp:11-21).
-inline uint64_t hash64(uint64_t key, uint64_t mask) {
-    key = (~key + (key << 21)) & mask;
-    key = key ^ key >> 24;
-    key = ((key + (key << 3)) + (key << 8)) & mask;
-    key = key ^ key >> 14;
-    key = ((key + (key << 2)) + (key << 4)) & mask;
-    key = key ^ key >> 28;
-    key = (key + (key << 31)) & mask;
-    return key;
-}
 
 // Cheap log2 for x >= 2 (include/mmpriv.h:12-20): exponent bits plus a
 // quadratic fit of the mantissa.

@@ -111,6 +111,7 @@ struct DevGraph {
     int32_t *e_from, *e_to, *e_w, *e_nin, *e_nout;
     int32_t *rank_to_id, *hlen, *tlen, *deg, *stk, *pre, *score;
     int32_t *hin, *hout, *stamp;  // heaviest in/out edge (first max in list order); fusion stamps
+    int32_t *csr_ptr, *csr_adj;   // topsort scratch: the view's out-lists, free until the view is rebuilt
     int32_t NC, EC;
 };
 
@@ -129,6 +130,7 @@ __device__ DevGraph slot_graph(char* s, const SlotLayout& L) {
     g.deg = (int32_t*)(s + L.deg); g.stk = (int32_t*)(s + L.stk); g.pre = (int32_t*)(s + L.pre);
     g.score = (int32_t*)(s + L.score);
     g.hin = (int32_t*)(s + L.hin); g.hout = (int32_t*)(s + L.hout); g.stamp = (int32_t*)(s + L.stamp);
+    g.csr_ptr = (int32_t*)(s + L.v_out_ptr); g.csr_adj = (int32_t*)(s + L.v_out_row);
     g.NC = L.NC; g.EC = L.EC;
     return g;
 }
@@ -465,10 +467,90 @@ __device__ void depth_jump(DevGraph& g, int nn, int pass, int32_t* arr, T* P, T*
 // heaviest-out-edge forests, computed by pointer jumping across the warp
 // (double-buffered in the slot's scratch arrays). Graphs too large for the
 // shared-memory budget use the sequential global-memory version.
+// The same LIFO Kahn order for graphs whose 16-bit lists do not fit the warp's
+// shared memory: out-lists as int32 CSR in the slot's view arrays, in-degree
+// counters (8 bits) and the stack (16 bits) in shared memory. Returns false
+// when an in-degree exceeds 255 or the stack outgrows its space; the caller
+// then sorts on the global lists, which recomputes every rank.
+__device__ bool topsort_large(DevGraph& g, int nn, uint8_t* sm, int sm_bytes, int lane) {
+    int32_t* optr = g.csr_ptr;
+    int32_t* adj = g.csr_adj;
+    uint8_t* deg = sm;
+    uint16_t* stk = reinterpret_cast<uint16_t*>(sm + ((nn + 15) & ~15));
+    const int cap = (sm_bytes - ((nn + 15) & ~15)) / 2;
+    int carry = 0;
+    bool big = false;
+    for (int c0 = 0; c0 < nn; c0 += 32) {
+        const int u = c0 + lane;
+        const int c = u < nn ? g.out_cnt[u] : 0;
+        int x = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (u < nn) optr[u] = carry + x - c;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) optr[nn] = carry;
+    for (int u = lane; u < nn; u += 32) {
+        int k = optr[u];
+        for (int e = g.out_head[u]; e >= 0; e = g.e_nout[e]) adj[k++] = g.e_to[e];
+        const int ic = g.in_cnt[u];
+        big |= ic > 255;
+        deg[u] = (uint8_t)ic;
+    }
+    if (__any_sync(0xffffffffu, big)) return false;
+    // zero in-degree seeds in id order
+    int sp = 0;
+    bool over = false;
+    for (int c0 = 0; c0 < nn; c0 += 32) {
+        const int u = c0 + lane;
+        const bool z = u < nn && deg[u] == 0;
+        const unsigned msk = __ballot_sync(0xffffffffu, z);
+        over |= sp + __popc(msk) > cap;
+        if (z && !over) stk[sp + __popc(msk & ((1u << lane) - 1u))] = (uint16_t)u;
+        sp += __popc(msk);
+    }
+    __syncwarp();
+    if (over) return false;
+    int nr = 0;
+    if (lane == 0) {
+        while (sp && !over) {
+            const int u = stk[--sp];
+            g.rank[u] = nr;
+            g.rank_to_id[nr++] = u;
+            const int k1 = optr[u + 1];
+            for (int k = optr[u]; k < k1; k++) {
+                const int v = adj[k];
+                const int dv = deg[v] - 1;
+                deg[v] = (uint8_t)dv;
+                if (dv == 0) {
+                    if (sp >= cap) { over = true; break; }
+                    stk[sp++] = (uint16_t)v;
+                }
+            }
+        }
+        if (!over) g.hdr[3] = nr;
+    }
+    over = __shfl_sync(0xffffffffu, over, 0);
+    __syncwarp();
+    return !over;
+}
+
 __device__ void dg_topsort_warp(DevGraph& g, int nn, int ne, bool with_lens, uint16_t* sm, int sm_bytes,
                                 int lane) {
     const size_t need = 2 * ((size_t)nn + 1) + 2 * (size_t)ne + 4 * (size_t)nn + 16;
     if (nn >= 65535 || ne >= 65535 || need > (size_t)sm_bytes) {
+        if (nn < 65535 && (size_t)nn + 16 + 2 * 256 <= (size_t)sm_bytes) {
+            if (topsort_large(g, nn, (uint8_t*)sm, sm_bytes, lane)) {
+                if (with_lens)
+                    for (int pass = 0; pass < 2; pass++)
+                        depth_jump<int32_t>(g, nn, pass, pass == 0 ? g.hlen : g.tlen, g.deg, g.stk, g.pre, g.score,
+                                            lane);
+                return;
+            }
+        }
         if (lane == 0) g.hdr[3] = dg_topsort(g, nn, with_lens);
         __syncwarp();
         return;

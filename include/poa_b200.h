@@ -213,7 +213,8 @@ int poa_align_noalloc(const poa_dev_window* w, const uint8_t* q_dev, int32_t qle
 /* Launch shape of the batch kernel (the autotuner's knobs): key 0 = blocks
  * per SM upper bound (the occupancy calculator still caps it), 1 = maximum
  * number of blocks in total (0 = no cap), 2 = shared memory per warp in
- * bytes (row ring + topsort workspace). Takes effect at the next run. */
+ * bytes, a multiple of 16 (row ring, staged records, query,
+ * topsort workspace). Takes effect at the next run. */
 int poa_batch_config(poa_ctx* ctx, int32_t key, int64_t value);
 
 /* Page-locked host memory (cudaMallocHost) for callers that want the

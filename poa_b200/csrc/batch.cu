@@ -825,6 +825,185 @@ __device__ __forceinline__ const int32_t* blk_src(const int32_t* ring, const int
     return st < 0 ? ring + (-st - 1) * RB * 16 : rs + st;
 }
 
+// One row of the warp fill: every chunk of 32 blocks (one block per lane) of
+// row i, whose descriptor is `cur` and whose predecessor records are
+// er_base[cur.e0 + k] in the backtrack's priority order. Predecessor blocks
+// come from blk_src (the shared-memory ring or the slot's row store). With
+// ARGMAX, each lane also keeps the first maximum of M over its cells.
+template <bool ARGMAX>
+__device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, const int4* __restrict__ er_base,
+                                         const int32_t* ring, int RB, const uint8_t* __restrict__ qsm, int i,
+                                         int lane, int32_t& bestM, int& bestJ) {
+    const Scoring sc = a.sc;
+    const int32_t K = add32(add32(NEG_INF, sc.e1), -sc.o1);
+    const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
+    const int d = cur.d;
+    int32_t* dst = const_cast<int32_t*>(blk_src(ring, a.rs, RB, cur.st));
+    const int nch = (bn + 31) >> 5;
+    int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
+    for (int c = 0; c < nch; c++) {
+        const int b = c * 32 + lane;
+        const bool act = b < bn;
+        const int B = Bs + b;
+        const int j0 = b * BLK;
+        int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
+        int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
+        bool c_blk = false, c_prev = false;
+        uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
+#pragma unroll
+        for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
+        if (act) {
+            const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
+            qlo = qw.x;
+            qhi = qw.y;
+            if (i == 0 && b == 0) Mpre[0] = 0;
+            for (int k = 0; k < d; k++) {
+                int pbsbe, pst, pbase;
+                if (k == 0) { pbsbe = cur.pbsbe; pst = cur.pst; pbase = cur.pbase; }
+                else { const int4 er = er_base[cur.e0 + k]; pbsbe = er.x; pst = er.y; pbase = er.w & 255; }
+                const int pBs = pbsbe & 0xffff, pBe = pbsbe >> 16;
+                const int32_t* src = blk_src(ring, a.rs, RB, pst);
+                const PredMask mk = pred_mask(B, pBs, pBe);
+                int32_t Mb[BLK], Db[BLK];
+                int32_t mprev = NEG_INF;
+                if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                if (mk.blk_in) {
+                    load_block16(src + (B - pBs) * 16, Mb, Db);
+                    uint8_t qc8[BLK];
+#pragma unroll
+                    for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qlo >> (8 * l)); qc8[4 + l] = (uint8_t)(qhi >> (8 * l)); }
+                    pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+                    if (d == 1) {
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
+                    }
+                }
+                if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
+            }
+        }
+        // prefix max of the scan keys across the warp
+        int32_t agg = INT_MIN;
+#pragma unroll
+        for (int l = 0; l < BLK; l++) {
+            H0[l] = mx(Mpre[l], Dv[l]);
+            agg = mx(agg, add32(H0[l], -(j0 + l) * sc.e1));
+        }
+        if (!act) agg = INT_MIN;
+        const int32_t incl = warp_incl_max(agg);
+        int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) P = INT_MIN;
+        P = mx(P, carryP);
+        const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
+        if (i == 0) {
+#pragma unroll
+            for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
+        } else {
+            int32_t run = P;
+#pragma unroll
+            for (int l = 0; l < BLK; l++) {
+                I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
+                M[l] = mx(H0[l], I[l]);
+                run = mx(run, add32(H0[l], -(j0 + l) * sc.e1));
+            }
+        }
+        if (ARGMAX && act) {
+#pragma unroll
+            for (int l = 0; l < BLK; l++)
+                if (M[l] > bestM) { bestM = M[l]; bestJ = j0 + l; }  // first maximum of the row
+        }
+        const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
+        const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
+        const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
+        const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
+        const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
+        if (act) {
+            if (d <= 1) {
+                uint32_t lo = 0, hi = 0;
+#pragma unroll
+                for (int l = 0; l < BLK; l++) {
+                    const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                    uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
+                    if (d == 1) {
+                        const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
+                        const bool inr = l == 0 ? c_prev : c_blk;
+                        const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
+                        const bool bm = cur.pbase == qc;
+                        const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                        if (eqM) r |= R_M4;
+                        if (eqM && bm && cur.w1ok) r |= R_M1;
+                        if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
+                        else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
+                    }
+                    if (l < 4) lo |= r << (8 * l);
+                    else hi |= r << (8 * (l - 4));
+                }
+                *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
+            } else {
+                // choices per cell: m1 | m4 << 16, dopen | dext << 16 (511 = none,
+                // 510 = the best matching predecessor failed the weight threshold)
+                uint32_t cm[BLK], cd[BLK];
+#pragma unroll
+                for (int l = 0; l < BLK; l++) { cm[l] = 0x01ff01ffu; cd[l] = 0x01ff01ffu; }
+                for (int k = 0; k < d; k++) {
+                    const int4 er = er_base[cur.e0 + k];
+                    const int pBs = er.x & 0xffff, pBe = er.x >> 16;
+                    const int32_t* src = blk_src(ring, a.rs, RB, er.y);
+                    const PredMask mk = pred_mask(B, pBs, pBe);
+                    if (!(mk.blk_in || mk.prev_in)) continue;
+                    const uint32_t pos = (uint32_t)er.z >> 16;
+                    const int pbase = er.w & 255;
+                    const uint32_t m1v = (er.w & 256) ? pos : 510u;
+                    int32_t Mb[BLK], Db[BLK];
+                    int32_t mprev = NEG_INF;
+                    if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                    if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
+                    else {
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                    }
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
+                        const bool inr = l == 0 ? mk.prev_in : mk.blk_in;
+                        const int32_t mv = l == 0 ? mprev : Mb[l > 0 ? l - 1 : 0];
+                        const bool bm = pbase == qc;
+                        const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                        if (eqM && (cm[l] >> 16) == 511u) cm[l] = (cm[l] & 0xffffu) | (pos << 16);
+                        if (eqM && bm && (cm[l] & 0xffffu) == 511u) cm[l] = (cm[l] & 0xffff0000u) | m1v;
+                        if (mk.blk_in) {
+                            if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
+                                cd[l] = (cd[l] & 0xffff0000u) | pos;
+                            if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
+                                cd[l] = (cd[l] & 0xffffu) | (pos << 16);
+                        }
+                    }
+                }
+                uint32_t r[BLK];
+#pragma unroll
+                for (int l = 0; l < BLK; l++) {
+                    const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                    uint32_t w = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
+                    uint32_t m1 = cm[l] & 0xffffu, m4 = cm[l] >> 16;
+                    if (m1 == 510u) m1 = W_NONE;
+                    uint32_t dd = cd[l] & 0xffffu;
+                    if (dd == 511u) {
+                        dd = cd[l] >> 16;
+                        if (dd != 511u) w |= W_DEXT;
+                    }
+                    r[l] = w | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
+                }
+                uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
+                tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
+                tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
+            }
+            store_block16(dst + b * 16, M, Dv);
+        }
+        carryP = mx(carryP, chunk_total);
+        carryM = nextM;
+        carryI = nextI;
+    }
+}
+
 __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__ desc, const int4* __restrict__ erec,
                                     int32_t* ring, int RB, const uint8_t* qsm, unsigned char* stage, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
@@ -851,168 +1030,10 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         const int4* er_base = staged ? serec - e_lo : erec;
         for (int i = i0; i < i0 + cnt; i++) {
             const RowDesc cur = sdesc[i - i0];
-            const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
-            const int d = cur.d;
-            int32_t* dst = const_cast<int32_t*>(blk_src(ring, a.rs, RB, cur.st));
-            cells += (int64_t)bn * BLK;
-            const int nch = (bn + 31) >> 5;
-            int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
-            for (int c = 0; c < nch; c++) {
-                const int b = c * 32 + lane;
-                const bool act = b < bn;
-                const int B = Bs + b;
-                const int j0 = b * BLK;
-                int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
-                int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
-                bool c_blk = false, c_prev = false;
-                uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
-#pragma unroll
-                for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
-                if (act) {
-                    const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
-                    qlo = qw.x;
-                    qhi = qw.y;
-                    if (i == 0 && b == 0) Mpre[0] = 0;
-                    for (int k = 0; k < d; k++) {
-                        int pbsbe, pst, pbase;
-                        if (k == 0) { pbsbe = cur.pbsbe; pst = cur.pst; pbase = cur.pbase; }
-                        else { const int4 er = er_base[cur.e0 + k]; pbsbe = er.x; pst = er.y; pbase = er.w & 255; }
-                        const int pBs = pbsbe & 0xffff, pBe = pbsbe >> 16;
-                        const int32_t* src = blk_src(ring, a.rs, RB, pst);
-                        const PredMask mk = pred_mask(B, pBs, pBe);
-                        int32_t Mb[BLK], Db[BLK];
-                        int32_t mprev = NEG_INF;
-                        if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
-                        if (mk.blk_in) {
-                            load_block16(src + (B - pBs) * 16, Mb, Db);
-                            uint8_t qc8[BLK];
-#pragma unroll
-                            for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qlo >> (8 * l)); qc8[4 + l] = (uint8_t)(qhi >> (8 * l)); }
-                            pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
-                            if (d == 1) {
-#pragma unroll
-                                for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
-                            }
-                        }
-                        if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
-                    }
-                }
-                // prefix max of the scan keys across the warp
-                int32_t agg = INT_MIN;
-#pragma unroll
-                for (int l = 0; l < BLK; l++) {
-                    H0[l] = mx(Mpre[l], Dv[l]);
-                    agg = mx(agg, add32(H0[l], -(j0 + l) * sc.e1));
-                }
-                if (!act) agg = INT_MIN;
-                const int32_t incl = warp_incl_max(agg);
-                int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
-                if (lane == 0) P = INT_MIN;
-                P = mx(P, carryP);
-                const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
-                if (i == 0) {
-#pragma unroll
-                    for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
-                } else {
-                    int32_t run = P;
-#pragma unroll
-                    for (int l = 0; l < BLK; l++) {
-                        I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
-                        M[l] = mx(H0[l], I[l]);
-                        run = mx(run, add32(H0[l], -(j0 + l) * sc.e1));
-                    }
-                }
-                const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
-                const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
-                const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
-                const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
-                const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
-                if (act) {
-                    if (d <= 1) {
-                        uint32_t lo = 0, hi = 0;
-#pragma unroll
-                        for (int l = 0; l < BLK; l++) {
-                            const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                            uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
-                            if (d == 1) {
-                                const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
-                                const bool inr = l == 0 ? c_prev : c_blk;
-                                const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
-                                const bool bm = cur.pbase == qc;
-                                const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
-                                if (eqM) r |= R_M4;
-                                if (eqM && bm && cur.w1ok) r |= R_M1;
-                                if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
-                                else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
-                            }
-                            if (l < 4) lo |= r << (8 * l);
-                            else hi |= r << (8 * (l - 4));
-                        }
-                        *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
-                    } else {
-                        // choices per cell: m1 | m4 << 16, dopen | dext << 16 (511 = none,
-                        // 510 = the best matching predecessor failed the weight threshold)
-                        uint32_t cm[BLK], cd[BLK];
-#pragma unroll
-                        for (int l = 0; l < BLK; l++) { cm[l] = 0x01ff01ffu; cd[l] = 0x01ff01ffu; }
-                        for (int k = 0; k < d; k++) {
-                            const int4 er = er_base[cur.e0 + k];
-                            const int pBs = er.x & 0xffff, pBe = er.x >> 16;
-                            const int32_t* src = blk_src(ring, a.rs, RB, er.y);
-                            const PredMask mk = pred_mask(B, pBs, pBe);
-                            if (!(mk.blk_in || mk.prev_in)) continue;
-                            const uint32_t pos = (uint32_t)er.z >> 16;
-                            const int pbase = er.w & 255;
-                            const uint32_t m1v = (er.w & 256) ? pos : 510u;
-                            int32_t Mb[BLK], Db[BLK];
-                            int32_t mprev = NEG_INF;
-                            if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
-                            if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
-                            else {
-#pragma unroll
-                                for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
-                            }
-#pragma unroll
-                            for (int l = 0; l < BLK; l++) {
-                                const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
-                                const bool inr = l == 0 ? mk.prev_in : mk.blk_in;
-                                const int32_t mv = l == 0 ? mprev : Mb[l > 0 ? l - 1 : 0];
-                                const bool bm = pbase == qc;
-                                const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
-                                if (eqM && (cm[l] >> 16) == 511u) cm[l] = (cm[l] & 0xffffu) | (pos << 16);
-                                if (eqM && bm && (cm[l] & 0xffffu) == 511u) cm[l] = (cm[l] & 0xffff0000u) | m1v;
-                                if (mk.blk_in) {
-                                    if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
-                                        cd[l] = (cd[l] & 0xffff0000u) | pos;
-                                    if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
-                                        cd[l] = (cd[l] & 0xffffu) | (pos << 16);
-                                }
-                            }
-                        }
-                        uint32_t r[BLK];
-#pragma unroll
-                        for (int l = 0; l < BLK; l++) {
-                            const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                            uint32_t w = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
-                            uint32_t m1 = cm[l] & 0xffffu, m4 = cm[l] >> 16;
-                            if (m1 == 510u) m1 = W_NONE;
-                            uint32_t dd = cd[l] & 0xffffu;
-                            if (dd == 511u) {
-                                dd = cd[l] >> 16;
-                                if (dd != 511u) w |= W_DEXT;
-                            }
-                            r[l] = w | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
-                        }
-                        uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
-                        tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
-                        tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
-                    }
-                    store_block16(dst + b * 16, M, Dv);
-                }
-                carryP = mx(carryP, chunk_total);
-                carryM = nextM;
-                carryI = nextI;
-            }
+            cells += (int64_t)((cur.bsbe >> 16) - (cur.bsbe & 0xffff) - 1) * BLK;
+            int32_t bm = 0;
+            int bj = 0;
+            fill_row<false>(a, cur, er_base, ring, RB, qsm, i, lane, bm, bj);
             __syncwarp();
         }
     }
@@ -1022,6 +1043,183 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         const int32_t* src = blk_src(ring, a.rs, RB, (int)last.st);
         a.out[1] = src[(jm / BLK) * 16 + jm % BLK];
         a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+        a.out[0] = ST_OK;
+    }
+    __syncwarp();
+}
+
+// Warp fill for bands known only row by row (adaptive band, -B; or the full
+// band, f = 0): the same chunk loop and records as the static fill
+// (fill_row), with each row's descriptor assembled when the row is reached:
+// its band from the adaptive state (row_band), its row-store location (a
+// full-width ring of ring_rows rows in the slot; rows with a successor
+// ring_rows or more rows ahead go to the spill area), its record offset (a
+// running sum), and its predecessor records with the predecessors' bands
+// and locations (staged in shared memory). After an adaptive row the warp
+// finds the first maximum of M and lane 0 updates the adaptive state
+// (src/align.cpp:1516-1568). out[4] / out[5]: record bytes and spilled
+// row-store entries used.
+constexpr int DYN_STAGE_EDGES = 128;
+
+// adaptive_update (dp_rowops.h, src/align.cpp:1516-1568) with the warp: the
+// predecessors' slope test and the successors' band updates run one lane per
+// edge (successors are distinct rows, so their updates do not collide); lane 0
+// settles row i's own state in between. Same results as the serial version.
+__device__ void adaptive_update_warp(const DpArgs& a, int i, int Bs, int max_j, int lane) {
+    const int n = a.v.n;
+    int32_t* Mp = a.state + AB_MP * n;
+    int32_t* Sl = a.state + AB_SL * n;
+    int32_t* Pl = a.state + AB_PL * n;
+    int32_t* Pr = a.state + AB_PR * n;
+    int32_t* Ol = a.state + AB_OL * n;
+    int32_t* Or = a.state + AB_OR * n;
+    int32_t* Ow = a.state + AB_OW * n;
+    const int max_acj = Bs * BLK + max_j;
+    const bool base_match = (int)a.v.base[i] == (int)a.qs[max_acj + 1];  // cur.base == seq[max_acj]
+    int sl_best = INT_MIN, max_slp = 0;
+    bool is_match = false;
+    if (base_match) {
+        const int e0 = a.v.in_ptr[i], e1 = a.v.in_ptr[i + 1];
+        for (int e = e0 + lane; e < e1; e += 32) {
+            const int p = a.v.in_row[e];
+            const int slp = Sl[p];
+            max_slp = max(max_slp, slp);
+            if (Mp[p] + 1 == max_acj) {
+                is_match = true;
+                sl_best = max(sl_best, slp + 1);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
+            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
+        }
+        is_match = __any_sync(0xffffffffu, is_match);
+    }
+    int sl_i = 0, ow_i = 0, ol_i = 0, or_i = 0;
+    if (lane == 0) {
+        Mp[i] = max_acj;
+        sl_i = Sl[i];
+        ow_i = Ow[i];
+        ol_i = Ol[i];
+        or_i = Or[i];
+        if (is_match) sl_i = mx(sl_i, sl_best);
+        if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
+        if (sl_i >= 30) {
+            ol_i = or_i = max_acj - a.v.hq_loc[i];
+            ow_i = 0;
+        }
+        Sl[i] = sl_i;
+        Ow[i] = ow_i;
+        Ol[i] = ol_i;
+        Or[i] = or_i;
+    }
+    sl_i = __shfl_sync(0xffffffffu, sl_i, 0);
+    ow_i = __shfl_sync(0xffffffffu, ow_i, 0);
+    ol_i = __shfl_sync(0xffffffffu, ol_i, 0);
+    or_i = __shfl_sync(0xffffffffu, or_i, 0);
+    const int o0 = a.v.out_ptr[i], o1 = a.v.out_ptr[i + 1];
+    for (int e = o0 + lane; e < o1; e += 32) {
+        const int s = a.v.out_row[e];
+        if (sl_i >= 30) {
+            Ol[s] = ol_i;
+            Or[s] = or_i;
+        } else {
+            Ol[s] = mn(Ol[s], ol_i);
+            Or[s] = mx(Or[s], or_i);
+        }
+        Pl[s] = mn(Pl[s], max_acj);
+        Pr[s] = mx(Pr[s], max_acj + 1);
+        Ow[s] = ow_i ? mx(Ow[s], ow_i) : ow_i;
+    }
+    __syncwarp();
+}
+
+__device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const int32_t* __restrict__ vmaxs,
+                                 const uint8_t* __restrict__ qsm, int4* sed, int lane) {
+    const int n = a.v.n, m = a.qlen + 1;
+    const bool adaptive = a.f > 0 && a.ab_band;
+    if (adaptive)
+        for (int r = lane; r < n; r += 32) adaptive_init_entry(a, r, m);
+    __syncwarp();
+    const int64_t ring_part = (int64_t)a.ring_rows * a.ring_blocks * 16;
+    int64_t st_next = ring_part, tb_next = 0, cells = 0;
+    for (int i = 0; i < n; i++) {
+        int Bs, Be;
+        row_band(a, i, m, Bs, Be);
+        if (i == 0) Bs = 0;
+        const int bn = Be - Bs - 1;
+        const int e0 = a.v.in_ptr[i];
+        const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
+        const int bpc = d >= 2 ? 4 : 1;
+        const bool spill = a.ring_rows <= 0 || (vmaxs[i] - i >= a.ring_rows) || bn > a.ring_blocks;
+        const int64_t row_st = spill ? st_next : (int64_t)(i % a.ring_rows) * a.ring_blocks * 16;
+        int st = ST_OK;
+        if (bn < 0) st = ST_DEGENERATE;
+        else if (d > MAX_MULTI_PRED) st = ST_INDEGREE;
+        else if ((spill && row_st + (int64_t)bn * 16 > a.rs_cap) || tb_next + (int64_t)bn * BLK * bpc > a.tb_cap ||
+                 row_st > INT_MAX || tb_next > INT_MAX)
+            st = ST_OOM;
+        if (st != ST_OK) {
+            if (lane == 0) a.out[0] = st;
+            __syncwarp();
+            return;
+        }
+        if (spill) st_next = row_st + (int64_t)bn * 16;
+        if (lane == 0) {
+            RowMeta rm;
+            rm.Bs = Bs; rm.Be = Be; rm.st = row_st; rm.tb = tb_next;
+            a.meta[i] = rm;
+        }
+        // predecessor records with the predecessors' bands and locations
+        int4* er = d <= DYN_STAGE_EDGES ? sed : erec + e0;
+        for (int k = lane; k < d; k += 32) {
+            int4 rec = erec[e0 + k];
+            const RowMeta pm = a.meta[rec.x];
+            rec.x = pm.Bs | (pm.Be << 16);
+            rec.y = (int32_t)pm.st;
+            er[k] = rec;
+        }
+        __syncwarp();
+        RowDesc cur;
+        cur.bsbe = Bs | (Be << 16);
+        cur.st = (int32_t)row_st;
+        cur.tb = (int32_t)tb_next;
+        cur.e0 = 0;
+        cur.d = d;
+        cur.ind = a.v.ind[i];
+        if (d >= 1) {
+            const int4 r0 = er[0];
+            cur.pbsbe = r0.x; cur.pst = r0.y; cur.pbase = r0.w & 255; cur.pw = r0.z & 0xffff;
+            cur.w1ok = (r0.w >> 8) & 1;
+            cur.prow0 = 0;
+        } else {
+            cur.pbsbe = cur.pst = cur.pbase = cur.pw = cur.w1ok = cur.prow0 = 0;
+        }
+        int32_t bestM = INT_MIN;
+        int bestJ = 0;
+        if (adaptive) fill_row<true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
+        else fill_row<false>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
+        cells += (int64_t)bn * BLK;
+        if (adaptive && i >= 1) {
+            // first maximum of the row: largest M, then smallest column
+            unsigned long long key = bestM == INT_MIN ? 0ull
+                                     : ((unsigned long long)((uint32_t)bestM ^ 0x80000000u) << 32) |
+                                           (unsigned long long)(0xffffffffu - (uint32_t)bestJ);
+            key = warp_max_u64(key);
+            const int max_j = bn > 0 ? (int)(0xffffffffu - (uint32_t)(key & 0xffffffffu)) : 0;
+            adaptive_update_warp(a, i, Bs, max_j, lane);
+        }
+        tb_next = (tb_next + (int64_t)bn * BLK * bpc + 15) & ~(int64_t)15;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        const RowMeta last = a.meta[n - 1];
+        const int jm = m - last.Bs * BLK;
+        a.out[1] = a.rs[last.st + (int64_t)(jm / BLK) * 16 + jm % BLK];
+        a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+        a.out[4] = (int32_t)tb_next;
+        a.out[5] = (int32_t)(st_next - ring_part);
         a.out[0] = ST_OK;
     }
     __syncwarp();
@@ -1113,7 +1311,7 @@ __device__ int bt_warp_static(const RowDesc* __restrict__ desc, const int32_t* _
 }
 
 // Build the DP rows of window [rank(source), rank(sink)] with the whole warp.
-__device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v, int lane) {
+__device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v, int lane, bool recs) {
     const int beg_i = g.rank[0], end_i = g.rank[1];
     const int n = end_i - beg_i + 1;
     int32_t* in_ptr = (int32_t*)(s + L.v_in_ptr);
@@ -1180,6 +1378,37 @@ __device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v,
         }
     }
     __syncwarp();
+    if (recs) {
+        // for the warp fill: each row's predecessor records in the backtrack's
+        // priority order (in_weight descending, in-list position ascending),
+        // erec = {predecessor row, 0, in_weight | position << 16,
+        //         base | (in_weight >= ind/10) << 8}; the fill patches in the
+        // predecessor's band and row-store location when it reaches the row.
+        // Also each row's furthest successor row (row-store placement).
+        int4* erec = (int4*)(s + L.v_pmeta);
+        int32_t* vmaxs = (int32_t*)(s + L.v_desc);
+        for (int r = lane; r < n; r += 32) {
+            const int e0 = in_ptr[r], d = r == 0 ? 0 : in_ptr[r + 1] - e0;
+            const int ind = vind[r];
+            for (int k = 0; k < d; k++) {
+                const int w = in_w[e0 + k];
+                const int4 rec = make_int4(in_row[e0 + k], 0, (w & 0xffff) | (k << 16),
+                                           (int)in_base[e0 + k] | ((w >= ind / 10) ? 256 : 0));
+                int at = k;
+                while (at > 0) {
+                    const int4 prev = erec[e0 + at - 1];
+                    if ((prev.z & 0xffff) >= w) break;  // ties keep list order
+                    erec[e0 + at] = prev;
+                    at--;
+                }
+                erec[e0 + at] = rec;
+            }
+            int maxs = r;
+            for (int k = out_ptr[r]; k < out_ptr[r + 1]; k++) maxs = max(maxs, out_row[k]);
+            vmaxs[r] = maxs;
+        }
+        __syncwarp();
+    }
     v.n = n;
     v.in_ptr = in_ptr; v.in_row = in_row; v.in_w = in_w; v.in_base = in_base;
     v.base = vb; v.ind = vind; v.hq = hq; v.hq_loc = hq_loc; v.tq = tq;
@@ -1251,7 +1480,7 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                                              A.sring_blocks, lane, beg_i);
             if (st != ST_OK) { status = st; break; }
         } else {
-            beg_i = build_view(g, s, L, v, lane);
+            beg_i = build_view(g, s, L, v, lane, true);
         }
         uint8_t* qs = (uint8_t*)(s + L.qs);
         const int64_t qsb = qs_bytes(len);
@@ -1289,7 +1518,18 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             dp_fill_warp_static(a, (const RowDesc*)(s + L.v_desc), (const int4*)(s + L.v_pmeta), (int32_t*)wsm,
                                 A.sring_blocks, qsm, stage, lane);
         } else {
-            dp_fill(grp, a);
+            // shared memory: staged records, and the query when it fits
+            const uint8_t* qf = qs;
+            int4* sed = reinterpret_cast<int4*>(wsm);
+            const int64_t sed_bytes = (int64_t)DYN_STAGE_EDGES * 16;
+            if (sed_bytes + qsb <= A.smem_per_warp) {
+                uint8_t* qsm = wsm + sed_bytes;
+                for (int64_t x = lane * 16; x < qsb; x += 32 * 16)
+                    *reinterpret_cast<uint4*>(qsm + x) = *reinterpret_cast<const uint4*>(qs + x);
+                qf = qsm;
+            }
+            __syncwarp();
+            dp_fill_warp_dyn(a, (int4*)(s + L.v_pmeta), (const int32_t*)(s + L.v_desc), qf, sed, lane);
         }
         __syncwarp();
         {
@@ -1312,13 +1552,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                 o[1] = a.out[3];
                 o[2] = v.n;
                 o[7] = v.n > 0 ? (int32_t)(mid * 1000 / ((long long)v.n * (len + 1))) : 0;
-                if constexpr (static_band) {
-                    o[4] = a.out[4];  // record bytes and spilled row-store entries (view scan)
-                    o[5] = a.out[5];
-                } else {
-                    o[4] = (int32_t)sr->tb_next;
-                    o[5] = (int32_t)(sr->st_next - (int64_t)L.ring_rows * L.ring_blocks * 16);
-                }
+                o[4] = a.out[4];  // record bytes and spilled row-store entries
+                o[5] = a.out[5];
             }
         }
         tick(PH_FILL);
@@ -1632,6 +1867,9 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     if (sring_rows < 2) sring_rows = 0;
     if (p_.f > 0 && !p_.ab_band && qsm_bytes + stage_bytes > smem_w)
         throw std::invalid_argument("reads too long for the batch kernel's shared memory; raise smem_per_warp");
+    if (!(p_.f > 0 && !p_.ab_band) && smem_w < DYN_STAGE_EDGES * 16)
+        throw std::invalid_argument("smem_per_warp too small for the adaptive-band fill");
+    if (smem_w % 16 != 0) throw std::invalid_argument("smem_per_warp must be a multiple of 16");
     int occ = 0;
     auto occ_of = [&](auto kern) {
         cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn), "smem attr");

@@ -348,7 +348,11 @@ int poa_batch_config(poa_ctx* ctx, int32_t key, int64_t value) {
     switch (key) {
         case 0: if (value < 1 || value > 32) return fail(ctx, POA_BAD_ARG, "blocks per SM"); ctx->batch->blocks_per_sm = (int32_t)value; break;
         case 1: if (value < 0) return fail(ctx, POA_BAD_ARG, "max blocks"); ctx->batch->max_blocks = (int32_t)value; break;
-        case 2: if (value < 1024 || value > 48 * 1024) return fail(ctx, POA_BAD_ARG, "smem per warp"); ctx->batch->smem_per_warp = (int32_t)value; break;
+        case 2:
+            if (value < 1024 || value > 48 * 1024 || value % 16 != 0)
+                return fail(ctx, POA_BAD_ARG, "smem per warp: 1024..49152 bytes, a multiple of 16");
+            ctx->batch->smem_per_warp = (int32_t)value;
+            break;
         default: return fail(ctx, POA_BAD_ARG, "unknown key");
     }
     return POA_OK;

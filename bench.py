@@ -246,9 +246,18 @@ def cpu_sample(ws, seconds, cores, binary, opts=(), chunk_per_core=4):
     return n / dt, n, dt, outs
 
 
-def make_windows(wl, rank, n):
+def make_windows(wl, rank, n, reads_per_window=0):
     from poa_b200 import synth
-    return getattr(synth, wl["gen"])(seed=shard_seed(rank, wl["seed"]), n_windows=n)
+    ws = getattr(synth, wl["gen"])(seed=shard_seed(rank, wl["seed"]), n_windows=n)
+    if reads_per_window > 0:
+        # small profiling captures: the first reads of every window
+        reads, offs = [], [0]
+        for w in range(ws.n_windows):
+            rs = ws.window_reads(w)[:reads_per_window]
+            reads.extend(rs)
+            offs.append(offs[-1] + len(rs))
+        ws = synth.pack_windows_from_reads(reads, offs)
+    return ws
 
 
 # --------------------------------------------------------------------- arms
@@ -258,7 +267,7 @@ def ours(args, world, rank, local, D):
     wl = WORKLOADS[args.workload]
     nwin = args.windows or wl["windows"]
     t0 = time.perf_counter()
-    ws = make_windows(wl, rank, nwin)
+    ws = make_windows(wl, rank, nwin, args.reads_per_window)
     log(f"[rank {rank}] generated {ws.n_windows} windows / {ws.n_reads} reads in {time.perf_counter() - t0:.1f}s")
     try:
         import torch
@@ -353,7 +362,9 @@ def ours(args, world, rank, local, D):
         "metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded; no dataset)",
-        "config": {"workload": wl["desc"], "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
+        "config": {"workload": wl["desc"] + (f" (first {args.reads_per_window} reads per window)"
+                                              if args.reads_per_window else ""),
+                   "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
                    "bases_per_rank": int(ws.seq.shape[0]), "mode": wl["mode"] if prop else
                    wl["mode"].replace(", learned band proposer sizes the slots", ""),
                    "parallelism": f"windows sharded over {world} GPU(s)",
@@ -443,6 +454,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-proposer", action="store_true", help="learned_band without the proposer's plan")
+    ap.add_argument("--reads-per-window", type=int, default=0,
+                    help="keep only the first N reads of each window (small profiling captures; 0 = all)")
     ap.add_argument("--max-blocks", type=int, default=0,
                     help="cap the persistent grid (small profiling captures); 0 = one full wave")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="batch kernel variant: 3 (default) or 4")

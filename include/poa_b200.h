@@ -15,7 +15,8 @@
  *   poa_align                     poa(), include/align.h:15, src/align.cpp:1353-1737
  *   poa_run                       the driver loop + output, src/main.cpp:84-126
  *                                 (alignment(), src/align.cpp:1741-1828; add_path,
- *                                 topsort, output_consensus / output_rc_msa,
+ *                                 topsort, output_consensus / output_rc_msa /
+ *                                 output_gfa,
  *                                 src/graph.cpp)
  *   poa_batch_*                   the same driver over many independent windows
  *                                 (no counterpart: the reference handles one
@@ -53,7 +54,7 @@ typedef struct {
     int32_t seeding;                            /* -S: 0 */
     int32_t k, mm_w, poa_w;                     /* -k -w -W: 19 10 0 (-W is read only when given) */
     int32_t thread;                             /* -t: 1 */
-    int32_t result;                             /* -r: 0 consensus, 1 row-column MSA */
+    int32_t result;                             /* -r: 0 consensus, 1 row-column MSA, 2 GFA */
     int32_t progressive;                        /* -p: 0 */
     int32_t verbose;                            /* -V: 0 */
 } poa_params;
@@ -104,8 +105,9 @@ int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end
 
 /* The whole minipoa run: reads in order, DP on the GPU, graph fusion on the
  * host, output text exactly as minipoa prints it (consensus FASTA for
- * result 0, one row per read for result 1). headers[i] is the text after '>'
- * of read i ("name comment"), or NULL / "" for ">i+1". *text is allocated
+ * result 0, one row per read for result 1, GFA for result 2, nothing for
+ * other values). headers[i] is the text after '>' of read i ("name
+ * comment"; GFA path lines use the name), or NULL / "" for ">i+1". *text is allocated
  * with malloc; release it with poa_free. scores (optional, nseq entries) gets
  * the end-cell score of each read's last poa() call (0 for the first read). */
 int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,

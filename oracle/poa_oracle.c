@@ -314,6 +314,80 @@ char *po_msa(const po_graph *g, int nseq, int *ncol) {
     return rows;
 }
 
+/* ------------------------------------------------------------------ GFA */
+typedef struct { char *a; size_t n, cap; } sbuf;
+static void sb_put(sbuf *b, const char *s) {
+    size_t k = strlen(s);
+    if (b->n + k + 1 > b->cap) {
+        b->cap = (b->n + k + 1) * 2;
+        b->a = (char *)realloc(b->a, b->cap);
+    }
+    memcpy(b->a + b->n, s, k + 1);
+    b->n += k;
+}
+
+/* graph::output_gfa, src/graph.cpp:358-434: H line; S and L lines in FIFO
+ * Kahn order from the source, stopping at the sink (L lines per in-edge in
+ * in-list order, source edges left out); read paths from each node's
+ * (read ord, position) pairs. A P line has no "\t*\n" when its read is empty
+ * (the reference writes the terminator only after the last position). */
+char *po_gfa(const po_graph *g, int nseq, const int *lens, const char *const *names) {
+    sbuf b = {0, 0, 0};
+    sb_put(&b, "");
+    if (g->n <= 2) return b.a;
+    int *deg = (int *)malloc(sizeof(int) * (size_t)g->n);
+    int *queue = (int *)malloc(sizeof(int) * (size_t)g->n);
+    int **paths = (int **)calloc((size_t)(nseq > 0 ? nseq : 1), sizeof(int *));
+    for (int i = 0; i < g->n; i++) deg[i] = g->node[i].in.n;
+    for (int i = 0; i < nseq; i++) paths[i] = (int *)calloc((size_t)(lens[i] > 0 ? lens[i] : 1), sizeof(int));
+    char line[128];
+    sb_put(&b, "H\tVN:Z:1.0\n");
+    int head = 0, tail = 0;
+    queue[tail++] = 0;
+    while (head < tail) {
+        const int cur = queue[head++];
+        if (cur == 1) break;
+        const po_node *v = &g->node[cur];
+        if (cur != 0) {
+            snprintf(line, sizeof line, "S\t%d\t%c\n", cur - 1, po_nt256[v->base]);
+            sb_put(&b, line);
+            for (int k = 0; k < v->in.n; k++) {
+                const int pre = v->in.a[k];
+                if (pre == 0) continue;
+                snprintf(line, sizeof line, "L\t%d\t+\t%d\t+\t0M\n", pre - 1, cur - 1);
+                sb_put(&b, line);
+            }
+            for (int k = 0; k < v->ids.n && k < v->idp.n; k++) {
+                const int id = v->ids.a[k], pos = v->idp.a[k];
+                if (id >= 0 && id < nseq && pos >= 0 && pos < lens[id]) paths[id][pos] = cur - 1;
+            }
+        }
+        for (int k = 0; k < v->out.n; k++) {
+            const int o = v->out.a[k];
+            if (--deg[o] == 0) queue[tail++] = o;
+        }
+    }
+    for (int i = 0; i < nseq; i++) {
+        if (names && names[i] && names[i][0]) {
+            sb_put(&b, "P\t");
+            sb_put(&b, names[i]);
+            sb_put(&b, "\t");
+        } else {
+            snprintf(line, sizeof line, "P\t%d\t", i + 1);
+            sb_put(&b, line);
+        }
+        for (int j = 0; j < lens[i]; j++) {
+            snprintf(line, sizeof line, "%d+%s", paths[i][j], j + 1 < lens[i] ? "," : "\t*\n");
+            sb_put(&b, line);
+        }
+    }
+    for (int i = 0; i < nseq; i++) free(paths[i]);
+    free(paths);
+    free(queue);
+    free(deg);
+    return b.a;
+}
+
 /* ------------------------------------------------------------------ poa() */
 enum { M_OP = 1, D_OP = 2, I_OP = 4, ALL_OP = 7 };
 

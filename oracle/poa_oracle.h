@@ -8,7 +8,8 @@
  * (src/align.cpp:1741-1756), graph fusion (src/graph.cpp:7-20, 170-235;
  * include/node.h:16-61), topological sort with hlen/tlen
  * (src/graph.cpp:21-128), consensus (src/graph.cpp:294-357) and the
- * row-column MSA (src/graph.cpp:237-251).
+ * row-column MSA (src/graph.cpp:237-251) and the GFA output
+ * (src/graph.cpp:358-434).
  *
  * Parity is pinned against the reference itself: tests/golden/ holds outputs
  * of the unmodified reference (built by oracle/Makefile into oracle/_ref/) on
@@ -66,6 +67,9 @@ void po_topsort(po_graph *g, const po_params *p, int op);
 char *po_consensus(const po_graph *g, int *len);
 /* Row-column MSA: nseq rows of *ncol chars, row r for ord r (malloc'd block). */
 char *po_msa(const po_graph *g, int nseq, int *ncol);
+/* GFA text (-r 2, src/graph.cpp:358-434); lens/names per read in input order
+ * (names may be NULL: reads are then numbered from 1). malloc'd. */
+char *po_gfa(const po_graph *g, int nseq, const int *lens, const char *const *names);
 
 /* Whole driver loop (src/main.cpp:84-126, default read order, no seeding).
  * seqs: ASCII. mode 0 = consensus, 1 = MSA. Returns malloc'd text exactly as

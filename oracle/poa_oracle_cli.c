@@ -1,7 +1,7 @@
 /*
  * poa_oracle_cli.c - command-line front end of the CPU restatement
  * (TEST INFRASTRUCTURE). Mirrors the subset of minipoa's CLI that the hot
- * path covers (src/main.cpp:14-35): -M -X -O -E -b -f -B -r {0,1}.
+ * path covers (src/main.cpp:14-35): -M -X -O -E -b -f -B -r {0,1,2}.
  * With -d FILE it also writes one record per read:
  *   A <read index> <score> <path length>
  *   <from>,<base>,<aligned_id> ...
@@ -85,7 +85,7 @@ int main(int argc, char **argv) {
         else if (!strcmp(o, "-d") && a + 1 < argc) dump = argv[++a];
         else in = o;
     }
-    if (!in) { fprintf(stderr, "usage: poa_oracle in.fa [-B] [-r 0|1] [-M -X -O -E -b -f] [-d dump]\n"); return 2; }
+    if (!in) { fprintf(stderr, "usage: poa_oracle in.fa [-B] [-r 0|1|2] [-M -X -O -E -b -f] [-d dump]\n"); return 2; }
     po_params_normalize(&p);
     int n;
     rec *r = read_fasta(in, &n);
@@ -115,6 +115,15 @@ int main(int argc, char **argv) {
         char *c = po_consensus(g, &len);
         printf(">consensus sequence\n%s\n", c);
         free(c);
+    } else if (mode == 2) {
+        int *lens = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+        const char **names = (const char **)malloc(sizeof(char *) * (size_t)(n > 0 ? n : 1));
+        for (int i = 0; i < n; i++) { lens[i] = r[i].len; names[i] = r[i].name; }
+        char *t = po_gfa(g, n, lens, names);
+        fputs(t, stdout);
+        free(t);
+        free(lens);
+        free((void *)names);
     } else {
         int nc;
         char *rows = po_msa(g, n, &nc);

@@ -56,7 +56,7 @@ class Params:
     mm_w: int = 10          # -w
     poa_w: int = 0          # -W (minipoa reads it only when given; 0 = unset)
     thread: int = 1         # -t
-    result: int = 0         # -r (0 consensus, 1 MSA)
+    result: int = 0         # -r (0 consensus, 1 MSA, 2 GFA)
     progressive: bool = False  # -p
     verbose: int = 0        # -V
 

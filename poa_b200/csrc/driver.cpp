@@ -140,9 +140,15 @@ int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
             text += rows[rid_to_ord[i]];
             text += "\n";
         }
-    } else {
-        return ST_BAD_ARG;
-    }
+    } else if (p.result == 2) {  // src/graph.cpp:358-434; names are the first word of each header
+        std::vector<int32_t> lens(nseq);
+        std::vector<std::string> names(nseq);
+        for (int i = 0; i < nseq; i++) {
+            lens[i] = (int32_t)seqs[i].size();
+            if (i < (int)headers.size()) names[i] = headers[i].substr(0, headers[i].find(' '));
+        }
+        g.gfa_text(lens, names, rid_to_ord, text);
+    }  // other values print nothing, as in src/main.cpp:124-126
     return ST_OK;
 }
 

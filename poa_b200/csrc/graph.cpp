@@ -283,4 +283,53 @@ void moves_to_path(const Graph& g, const HostWindow& w, const int32_t* moves, in
     }
 }
 
+// graph::output_gfa, src/graph.cpp:358-434. Segments and links come out in
+// FIFO Kahn order from the source, which stops at the sink; links follow each
+// node's in-list (edges from the source are not written). A read's path is
+// its node per position, from the (read ord, position) pairs its nodes carry.
+// A read with no bases gets "P\t<name>\t" and no line end, as in the
+// reference, which writes the terminator after the last position only.
+void Graph::gfa_text(const std::vector<int32_t>& read_len, const std::vector<std::string>& names,
+                     const std::vector<int32_t>& rid_to_ord, std::string& out) const {
+    out.clear();
+    const int n = (int)node.size();
+    if (n <= 2) return;
+    const int nseq = (int)read_len.size();
+    std::vector<int32_t> deg(n);
+    for (int i = 0; i < n; i++) deg[i] = (int32_t)node[i].in.size();
+    std::vector<std::vector<int32_t>> paths(nseq);
+    for (int i = 0; i < nseq; i++) paths[i].assign(read_len[rid_to_ord[i]], 0);
+    out += "H\tVN:Z:1.0\n";
+    std::vector<int32_t> fifo;
+    fifo.reserve(n);
+    fifo.push_back(0);
+    for (size_t head = 0; head < fifo.size(); head++) {
+        const int cur = fifo[head];
+        if (cur == 1) break;
+        const Node& v = node[cur];
+        if (cur != 0) {
+            out += "S\t" + std::to_string(cur - 1) + "\t" + kNt256[v.base] + "\n";
+            for (int32_t pre : v.in)
+                if (pre != 0) out += "L\t" + std::to_string(pre - 1) + "\t+\t" + std::to_string(cur - 1) + "\t+\t0M\n";
+            for (size_t k = 0; k < v.ids.size() && k < v.idp.size(); k++) {
+                const int id = v.ids[k], pos = v.idp[k];
+                if (id >= 0 && id < nseq && pos >= 0 && pos < (int)paths[id].size()) paths[id][pos] = cur - 1;
+            }
+        }
+        for (int32_t o : v.out)
+            if (--deg[o] == 0) fifo.push_back(o);
+    }
+    for (int i = 0; i < nseq; i++) {
+        out += "P\t";
+        out += (i < (int)names.size() && !names[i].empty()) ? names[i] : std::to_string(i + 1);
+        out += "\t";
+        const std::vector<int32_t>& pth = paths[rid_to_ord[i]];
+        const int len = (int)paths[i].size();
+        for (int j = 0; j < len; j++) {
+            out += std::to_string(j < (int)pth.size() ? pth[j] : 0);
+            out += j + 1 < len ? "+," : "+\t*\n";
+        }
+    }
+}
+
 }  // namespace pb

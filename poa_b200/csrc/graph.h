@@ -38,6 +38,10 @@ class Graph {
     void topsort(bool with_lens, bool seeding, int op);               // src/graph.cpp:21-128
     void build_consensus(bool need_coverages);                        // src/graph.cpp:294-351
     std::vector<std::string> msa_rows(int nseq) const;                // src/graph.cpp:237-251
+    // GFA text, src/graph.cpp:358-434; read_len / names by input index,
+    // rid_to_ord maps them to the read ord used in the graph.
+    void gfa_text(const std::vector<int32_t>& read_len, const std::vector<std::string>& names,
+                  const std::vector<int32_t>& rid_to_ord, std::string& out) const;
 
     std::vector<Node> node;
     std::vector<int32_t> rank;        // rank -> node id

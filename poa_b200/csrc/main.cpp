@@ -3,10 +3,10 @@
 // GPU through the C ABI (include/poa_b200.h).
 //
 //   minipoa_b200 in.fa[.gz] [-M 2] [-X -4] [-O -4] [-E -2] [-b 100] [-f 40] [-B]
-//                [-S] [-k 19] [-w 10] [-W 10000] [-t 1] [-r 0|1] [-V 0]
+//                [-S] [-k 19] [-w 10] [-W 10000] [-t 1] [-r 0|1|2] [-V 0]
 //
 // Reads FASTA/FASTQ, optionally gzip-compressed (src/handle_input.cpp:13-43).
-// -r 0 prints the consensus, -r 1 the row-column MSA. Exit codes follow the
+// -r 0 prints the consensus, -r 1 the row-column MSA, -r 2 the graph as GFA. Exit codes follow the
 // reference: a backtrack that leaves the band exits 0 with no output
 // (src/align.cpp:1584-1588), a backtrack error exits 1 (src/align.cpp:1730).
 #include <zlib.h>
@@ -86,7 +86,7 @@ void usage() {
                  "  -w, --mm_w INT         minimizer window [10]\n"
                  "  -W, --poa_w INT        minimum distance between anchors [unset]\n"
                  "  -t, --thread INT       threads [1]\n"
-                 "  -r, --result INT       0 consensus, 1 row-column MSA [0]\n"
+                 "  -r, --result INT       0 consensus, 1 row-column MSA, 2 GFA [0]\n"
                  "  -V, --verbose INT      verbose level [0]\n"
                  "  -h, --help             this help\n";
 }
@@ -141,10 +141,6 @@ int main(int argc, char** argv) {
             break;
         }
         if (!done) { std::cerr << "error parsing options: unknown option " << o << "\n"; return 1; }
-    }
-    if (p.result != 0 && p.result != 1) {
-        std::cerr << "result format " << p.result << " is not supported by minipoa_b200\n";
-        return 1;
     }
     std::string data;
     if (!path.empty() && !read_all(path.c_str(), data)) {

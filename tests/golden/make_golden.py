@@ -7,7 +7,7 @@ reference's own sources into ``oracle/_ref/``):
     python tests/golden/make_golden.py --fullsize   # md5 of full-size runs
 
 For every case it writes ``<case>.fa`` (seeded synthetic input),
-``<case>.out`` (the reference CLI's stdout, byte for byte) and, where the case
+``<case>.out`` (the reference CLI's stdout, byte for byte: consensus, MSA or GFA) and, where the case
 has per-call records, ``<case>.dump`` (one score + path per alignment() call,
 from ``oracle/ref_harness``). ``manifest.json`` lists the cases and options.
 The fixtures are kept small so the CPU test-suite stays fast; the full-size
@@ -69,9 +69,13 @@ def cases():
         out.append((name, reads, [], True))
         out.append((name + "_adaptive", reads, ["-B"], False))
         out.append((name + "_msa", reads, ["-r", "1"], False))
+        out.append((name + "_gfa", reads, ["-r", "2"], False))
     seed_in = synth.single_graph_msa(seed=17, nseq=10, length=3000)
     out.append(("seeded_msa", seed_in, ["-S", "-r", "1"], False))
     out.append(("seeded_cons", seed_in, ["-S"], False))
+    out.append(("seeded_gfa", seed_in, ["-S", "-r", "2"], False))
+    out.append(("gfa_small", synth.single_graph_msa(seed=19, nseq=8, length=600), ["-r", "2"], False))
+    out.append(("gfa_adaptive", noisy, ["-B", "-r", "2"], False))
     return out
 
 

@@ -99,7 +99,6 @@ int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
                   std::vector<int32_t>* scores, RunStats* stats) {
     (void)stats;
     const int nseq = (int)seqs.size();
-    if (p.progressive) return ST_UNSUPPORTED;  // the -p guide tree is not restated
     Graph g;
     std::vector<int32_t> ord(nseq);
     std::iota(ord.begin(), ord.end(), 0);

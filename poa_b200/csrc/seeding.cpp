@@ -410,7 +410,74 @@ void Seeder::init(const Params& p, const std::vector<std::string>& seqs) {
     }
 }
 
-void Seeder::guide_tree(const Params&) {}
+// minimizer_t::get_guide_tree, src/minimizer.cpp:195-386: the progressive read
+// order of -p. Shared minimizers per read pair (for every hash, the smaller of
+// the two reads' counts), a length-weighted Jaccard similarity per ordered
+// pair, the most similar pair first, then repeatedly the read with the largest
+// similarity sum to the reads already ordered (first maximum wins). Pairs are
+// counted over the reads present in each hash group only, which adds the same
+// totals as the reference's loop over all pairs.
+void Seeder::guide_tree(const Params& p) {
+    const int n = nseq_;
+    if (!p.progressive || n < 2 || mm_.empty()) return;
+    std::vector<Anchor> mm = mm_;
+    std::sort(mm.begin(), mm.end(), [](const Anchor& a, const Anchor& b) { return a.x < b.x; });
+    auto tri = [](int64_t hi, int64_t lo) { return ((hi * (hi + 1)) >> 1) + lo; };
+    std::vector<int32_t> hit((size_t)tri(n - 1, n - 1) + 1, 0);
+    std::vector<int32_t> cnt(n, 0), present;
+    for (size_t a = 0; a < mm.size();) {
+        size_t b = a;
+        while (b < mm.size() && mm[b].x == mm[a].x) b++;
+        present.clear();
+        for (size_t j = a; j < b; j++) {
+            const int r = (int)(mm[j].y >> 32);
+            if (cnt[r]++ == 0) present.push_back(r);
+            hit[tri(r, r)]++;
+        }
+        for (size_t u = 0; u < present.size(); u++)
+            for (size_t v = u + 1; v < present.size(); v++) {
+                const int r1 = std::min(present[u], present[v]), r2 = std::max(present[u], present[v]);
+                hit[tri(r2, r1)] += std::min(cnt[r1], cnt[r2]);
+            }
+        for (int r : present) cnt[r] = 0;
+        a = b;
+    }
+    std::vector<double> jac((size_t)n * n, 0.0);
+    double max_jac = -1.0;
+    int max_i = -1, max_j = -1;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+            if (i == j) continue;
+            const int shared = i > j ? hit[tri(i, j)] : hit[tri(j, i)];
+            const int tot = hit[tri(i, i)] + hit[tri(j, j)] - shared;
+            double v = 0.0;
+            if (tot > 0) {
+                v = (0.0 + shared) / tot;
+                v = v * ((0.51 * len_[i] / maxl_) + (0.49 * len_[j] / maxl_));
+            }
+            jac[(size_t)i * n + j] = v;
+            if (v > max_jac) { max_jac = v; max_i = i; max_j = j; }
+        }
+    std::vector<char> in_ord(n, 0);
+    ord[0] = max_i;
+    ord[1] = max_j;
+    rid_to_ord[max_i] = 0;
+    rid_to_ord[max_j] = 1;
+    in_ord[max_i] = in_ord[max_j] = 1;
+    for (int k = 2; k < n; k++) {
+        double best = -1.0;
+        int pick = n;
+        for (int r2 = 0; r2 < n; r2++) {
+            if (in_ord[r2]) continue;  // the reference scores it -1, which never wins
+            double sum = 0.0;
+            for (int t = 0; t < k; t++) sum += jac[(size_t)ord[t] * n + r2];
+            if (sum > best) { best = sum; pick = r2; }
+        }
+        ord[k] = pick;
+        rid_to_ord[pick] = k;
+        in_ord[pick] = 1;
+    }
+}
 
 // src/minimizer.cpp:404-442: same-hash minimizer pairs of target tid and
 // query qid; anchors sorted by target position

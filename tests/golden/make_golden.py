@@ -76,6 +76,14 @@ def cases():
     out.append(("seeded_gfa", seed_in, ["-S", "-r", "2"], False))
     out.append(("gfa_small", synth.single_graph_msa(seed=19, nseq=8, length=600), ["-r", "2"], False))
     out.append(("gfa_adaptive", noisy, ["-B", "-r", "2"], False))
+    prog = synth.single_graph_msa(seed=23, nseq=12, length=1500)
+    out.append(("prog_msa", prog, ["-p", "-r", "1"], False))
+    out.append(("prog_cons", prog, ["-p"], False))
+    # no "-p -r 2" case: the reference aborts there (output_gfa sizes each path by
+    # rid_to_ord but fills it by read ord, src/graph.cpp:369, 397-401)
+    out.append(("prog_adaptive", noisy, ["-p", "-B"], False))
+    out.append(("prog_seeded_msa", seed_in, ["-p", "-S", "-r", "1"], False))
+    out.append(("prog_edge", edge_reads()["edge_mixed"], ["-p", "-r", "1"], False))
     return out
 
 

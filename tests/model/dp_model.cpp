@@ -210,6 +210,7 @@ int model_run(int nseq, const char* const* seqs, const int* lens, const int* par
     Params p;
     p.match = params[0]; p.mismatch = params[1]; p.gap_open1 = params[2]; p.gap_ext1 = params[3];
     p.b = params[4]; p.f = params[5]; p.ab_band = params[6]; p.result = params[7]; p.enable_seeding = params[8];
+    p.progressive = params[9];
     normalize_params(p);
     std::vector<std::string> s(nseq), headers;
     for (int i = 0; i < nseq; i++) s[i].assign(seqs[i], lens[i]);

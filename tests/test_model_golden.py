@@ -43,15 +43,15 @@ def model():
 
 
 def opts_to_params(opts):
-    p = dict(M=2, X=-4, O=-4, E=-2, b=100, f=40, B=0, r=0, S=0)
+    p = dict(M=2, X=-4, O=-4, E=-2, b=100, f=40, B=0, r=0, S=0, p=0)
     it = iter(opts)
     for o in it:
         k = o.lstrip("-")
-        if k in ("B", "S"):
+        if k in ("B", "S", "p"):
             p[k] = 1
         else:
             p[k] = int(next(it))
-    return [p["M"], p["X"], p["O"], p["E"], p["b"], p["f"], p["B"], p["r"], p["S"]]
+    return [p["M"], p["X"], p["O"], p["E"], p["b"], p["f"], p["B"], p["r"], p["S"], p["p"]]
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
@@ -60,7 +60,7 @@ def test_model_matches_reference(case, model):
     n = len(seqs)
     arr = (ctypes.c_char_p * n)(*seqs)
     lens = (ctypes.c_int * n)(*[len(s) for s in seqs])
-    par = (ctypes.c_int * 9)(*opts_to_params(case["opts"]))
+    par = (ctypes.c_int * 10)(*opts_to_params(case["opts"]))
     out = ctypes.c_void_p()
     scores = (ctypes.c_int * (n + 1))()
     st = model.model_run(n, arr, lens, par, ctypes.byref(out), scores, n + 1)

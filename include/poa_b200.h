@@ -112,6 +112,14 @@ int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end
  * the end-cell score of each read's last poa() call (0 for the first read). */
 int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
             const char* const* headers, char** text, size_t* text_len, int32_t* scores);
+/* poa_run on top of an existing graph, minipoa -i (read_gfa,
+ * src/handle_input.cpp:444-494; src/main.cpp:86-126): gfa holds the GFA
+ * text (S lines become nodes, P lines reads without bases; L/W lines are
+ * ignored); the reads then extend that graph. The outputs list the GFA's
+ * paths first, as the reference does. A malformed GFA returns POA_BAD_ARG
+ * with the reason in poa_last_error. */
+int poa_run_gfa(poa_ctx* ctx, const char* gfa, size_t gfa_len, int32_t nseq, const char* const* seqs,
+                const int32_t* lens, const char* const* headers, char** text, size_t* text_len, int32_t* scores);
 
 /* Batched windows (consensus mode, no -S/-p): many independent read sets,
  * one POA graph and one consensus each, all in one persistent launch on the

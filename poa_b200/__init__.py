@@ -73,7 +73,9 @@ class Params:
         p = cls()
         it = iter(opts)
         for o in it:
-            if o in flags:
+            if o == "-i":
+                next(it)  # the graph file: see Context.run_gfa
+            elif o in flags:
                 setattr(p, flags[o], True)
             elif o in keys:
                 setattr(p, keys[o], int(next(it)))
@@ -107,6 +109,11 @@ def lib() -> ctypes.CDLL:
                           ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
                           ctypes.POINTER(ctypes.c_int32)]
     L.poa_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+    L.poa_run_gfa.restype = ctypes.c_int
+    L.poa_run_gfa.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int32,
+                              ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int32),
+                              ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_void_p),
+                              ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int32)]
     _i64p, _i32p, _u8p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), ctypes.c_void_p
     L.poa_batch_upload.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int64, _i64p, _i32p, ctypes.c_int32, _i32p,
                                    ctypes.c_int32]
@@ -183,6 +190,24 @@ class Context:
         olen = ctypes.c_size_t()
         scores = (ctypes.c_int32 * max(n, 1))()
         st = lib().poa_run(self._h, n, arr, lens, hdr, ctypes.byref(out), ctypes.byref(olen), scores)
+        self._check(st)
+        text = ctypes.string_at(out.value, olen.value)
+        lib().poa_free(out)
+        return text, list(scores)[:n]
+
+    def run_gfa(self, gfa: bytes, seqs: Sequence[bytes], headers: Optional[Sequence[str]] = None):
+        """minipoa -i: extend the graph in ``gfa`` (GFA text) with ``seqs``; returns (text, scores)."""
+        n = len(seqs)
+        arr = (ctypes.c_char_p * max(n, 1))(*[bytes(s) for s in seqs])
+        lens = (ctypes.c_int32 * max(n, 1))(*[len(s) for s in seqs])
+        hdr = None
+        if headers is not None:
+            hdr = (ctypes.c_char_p * max(n, 1))(*[h.encode() for h in headers])
+        out = ctypes.c_void_p()
+        olen = ctypes.c_size_t()
+        scores = (ctypes.c_int32 * max(n, 1))()
+        g = bytes(gfa)
+        st = lib().poa_run_gfa(self._h, g, len(g), n, arr, lens, hdr, ctypes.byref(out), ctypes.byref(olen), scores)
         self._check(st)
         text = ctypes.string_at(out.value, olen.value)
         lib().poa_free(out)

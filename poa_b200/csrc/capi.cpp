@@ -212,8 +212,10 @@ int poa_align(poa_ctx* ctx, const poa_graph_view* g, int32_t beg_id, int32_t end
     }
 }
 
-int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
-            const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
+namespace {
+
+int run_impl(poa_ctx* ctx, const std::string* gfa, int32_t nseq, const char* const* seqs, const int32_t* lens,
+             const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
     if (!ctx || nseq < 0 || (nseq > 0 && (!seqs || !lens)) || !text) return fail(ctx, POA_BAD_ARG, "null argument");
     try {
         std::vector<std::string> s(nseq), h;
@@ -227,8 +229,8 @@ int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* 
         }
         std::string out;
         std::vector<int32_t> sc;
-        int st = pb::run_reads(ctx->p, s, h, *ctx->eng, out, scores ? &sc : nullptr, nullptr);
-        if (st != POA_OK) return fail(ctx, st, poa_status_str(st));
+        int st = pb::run_reads(ctx->p, s, h, *ctx->eng, out, scores ? &sc : nullptr, nullptr, gfa);
+        if (st != POA_OK) return fail(ctx, st, out.empty() ? std::string(poa_status_str(st)) : out);
         char* buf = (char*)std::malloc(out.size() + 1);
         if (!buf) return fail(ctx, POA_BAD_ARG, "host allocation failed");
         std::memcpy(buf, out.data(), out.size());
@@ -244,6 +246,20 @@ int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* 
     } catch (const std::exception& e) {
         return fail(ctx, POA_CUDA, e.what());
     }
+}
+
+}  // namespace
+
+int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* lens,
+            const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
+    return run_impl(ctx, nullptr, nseq, seqs, lens, headers, text, text_len, scores);
+}
+
+int poa_run_gfa(poa_ctx* ctx, const char* gfa, size_t gfa_len, int32_t nseq, const char* const* seqs,
+                const int32_t* lens, const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
+    if (!gfa && gfa_len > 0) return fail(ctx, POA_BAD_ARG, "null GFA text");
+    const std::string g(gfa ? gfa : "", gfa_len);
+    return run_impl(ctx, &g, nseq, seqs, lens, headers, text, text_len, scores);
 }
 
 int poa_batch_upload(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,

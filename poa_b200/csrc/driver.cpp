@@ -5,6 +5,7 @@
 #include "driver.h"
 
 #include <numeric>
+#include <unordered_map>
 
 #include "seeding.h"
 
@@ -94,12 +95,102 @@ int32_t alignment(const Params& p, Graph& g, Seeder* seeder, int rid, const uint
     return ST_OK;
 }
 
-int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
-                  const std::vector<std::string>& headers, DpEngine& eng, std::string& text,
-                  std::vector<int32_t>* scores, RunStats* stats) {
+int32_t load_gfa(const Params& p, const std::string& text, Graph& g, std::vector<std::string>& path_names,
+                 std::string& err) {
+    std::unordered_map<std::string, int> seg;  // segment name -> index
+    std::vector<int32_t> seg_first, seg_last;  // its first / last node id
+    size_t pos = 0;
+    while (pos < text.size()) {
+        size_t eol = text.find('\n', pos);
+        if (eol == std::string::npos) eol = text.size();
+        std::string line = text.substr(pos, eol - pos);
+        pos = eol + 1;
+        if (!line.empty() && line.back() == '\r') line.pop_back();
+        if (line.size() < 3 || line[1] != '\t') continue;
+        if (line[0] != 'S' && line[0] != 'P') continue;
+        // the first two tab-separated fields after the record type
+        std::vector<std::string> f;
+        size_t a = 2;
+        while (f.size() < 2) {
+            size_t t = line.find('\t', a);
+            if (t == std::string::npos) { f.push_back(line.substr(a)); break; }
+            f.push_back(line.substr(a, t - a));
+            a = t + 1;
+        }
+        if (f.size() < 2) {
+            err = line[0] == 'S' ? "no seq in GFA segment line (" + f[0] + ")" : "no path in GFA path line (" + f[0] + ")";
+            return ST_BAD_ARG;
+        }
+        if (line[0] == 'S') {  // gfa_parse_S, src/handle_input.cpp:78-128
+            if (seg.count(f[0])) { err = "duplicated segment " + f[0]; return ST_BAD_ARG; }
+            if (f[1].empty()) { err = "empty segment " + f[0]; return ST_BAD_ARG; }
+            seg[f[0]] = (int)seg_first.size();
+            int first = -1, last = -1;
+            for (char c : f[1]) {
+                last = g.add_node(nt4((uint8_t)c));
+                if (first < 0) first = last;
+            }
+            seg_first.push_back(first);
+            seg_last.push_back(last);
+            continue;
+        }
+        // gfa_parse_P, src/handle_input.cpp:129-246: "name+,name+,..." (or all '-')
+        const int pid = (int)path_names.size();
+        const std::string& walk = f[1];
+        int is_rc = -1, last_id = 0, next_id = 1, cur_pos = 0;
+        size_t start = 0;
+        for (size_t k = 0; k < walk.size(); k++) {
+            const char c = walk[k];
+            if (c != '+' && c != '-') continue;
+            const std::string name = walk.substr(start, k - start);
+            const bool rc = c == '-';
+            if ((rc && is_rc == 0) || (!rc && is_rc == 1)) {
+                err = "path has both '+' and '-' segments (" + f[0] + ")";
+                return ST_BAD_ARG;
+            }
+            is_rc = rc ? 1 : 0;
+            auto it = seg.find(name);
+            if (it == seg.end()) { err = "segment " + name + " does not exist"; return ST_BAD_ARG; }
+            const int in_id = seg_first[it->second], out_id = seg_last[it->second];
+            if (!rc) {
+                g.add_adj(pid, last_id, in_id, cur_pos++);
+                for (int i = 0; i < out_id - in_id; i++) g.add_adj(pid, in_id + i, in_id + i + 1, cur_pos++);
+                last_id = out_id;
+            } else {
+                g.add_adj(pid, out_id, next_id, cur_pos++);
+                for (int i = 0; i < out_id - in_id; i++) g.add_adj(pid, in_id + i, in_id + i + 1, cur_pos++);
+                next_id = in_id;
+            }
+            start = k + 2;  // past the sign and the separator
+        }
+        if (is_rc != 0) g.add_adj(pid, 0, next_id, cur_pos++);  // also when no segment was signed, as in the reference
+        else g.add_adj(pid, last_id, 1, cur_pos++);
+        path_names.push_back(f[0]);
+    }
+    g.topsort(p.f > 0, p.enable_seeding != 0, 0);
+    return ST_OK;
+}
+
+int32_t run_reads(const Params& p, const std::vector<std::string>& reads,
+                  const std::vector<std::string>& read_headers, DpEngine& eng, std::string& text,
+                  std::vector<int32_t>* scores, RunStats* stats, const std::string* gfa) {
     (void)stats;
-    const int nseq = (int)seqs.size();
     Graph g;
+    // an existing graph's paths come first, as reads without bases (src/main.cpp:86-96)
+    std::vector<std::string> seqs, headers;
+    int exist = 0;
+    if (gfa) {
+        std::vector<std::string> names;
+        std::string err;
+        const int32_t st = load_gfa(p, *gfa, g, names, err);
+        if (st != ST_OK) { text = err; return st; }
+        exist = (int)names.size();
+        seqs.assign(exist, std::string());
+        for (const std::string& nm : names) headers.push_back(nm + " ");
+    }
+    seqs.insert(seqs.end(), reads.begin(), reads.end());
+    for (size_t i = 0; i < reads.size(); i++) headers.push_back(i < read_headers.size() ? read_headers[i] : "");
+    const int nseq = (int)seqs.size();
     std::vector<int32_t> ord(nseq);
     std::iota(ord.begin(), ord.end(), 0);
     std::vector<int32_t> rid_to_ord = ord;
@@ -108,7 +199,7 @@ int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
     if (p.enable_seeding || p.progressive) {
         sd.init(p, seqs);
         seeder = &sd;
-        if (p.progressive) {
+        if (p.progressive && !gfa) {  // no guide tree when extending a graph (src/main.cpp:101)
             sd.guide_tree(p);
             ord = sd.ord;
             rid_to_ord = sd.rid_to_ord;
@@ -116,7 +207,7 @@ int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
     }
     std::vector<Res> res;
     std::vector<uint8_t> q;
-    for (int i = 0; i < nseq; i++) {
+    for (int i = exist; i < nseq; i++) {
         int rid = ord[i];
         const std::string& s = seqs[rid];
         q.resize(s.size());

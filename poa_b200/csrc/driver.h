@@ -62,8 +62,19 @@ struct RunStats {
     int64_t cells = 0;
     int64_t dp_calls = 0;
 };
+// gfa (optional): the text of an existing graph to extend (-i, read_gfa,
+// src/handle_input.cpp:444-494). Its paths come first in the outputs (as
+// reads without bases), then the reads of seqs.
 int32_t run_reads(const Params& p, const std::vector<std::string>& seqs,
                   const std::vector<std::string>& headers, DpEngine& eng, std::string& text,
-                  std::vector<int32_t>* scores, RunStats* stats);
+                  std::vector<int32_t>* scores, RunStats* stats, const std::string* gfa = nullptr);
+
+// read_gfa, src/handle_input.cpp:444-494: S lines add one node per base of the
+// segment, P lines add their walk as a read (edges with the read's ord, in
+// walk order; '-' walks linked from the sink side as the reference does); L
+// and W lines are ignored; then an op-0 topsort. On error returns ST_BAD_ARG
+// with the reason in err.
+int32_t load_gfa(const Params& p, const std::string& text, Graph& g, std::vector<std::string>& path_names,
+                 std::string& err);
 
 }  // namespace pb

@@ -3,10 +3,11 @@
 // GPU through the C ABI (include/poa_b200.h).
 //
 //   minipoa_b200 in.fa[.gz] [-M 2] [-X -4] [-O -4] [-E -2] [-b 100] [-f 40] [-B]
-//                [-S] [-k 19] [-w 10] [-W 10000] [-t 1] [-r 0|1|2] [-V 0]
+//                [-S] [-p] [-k 19] [-w 10] [-W 10000] [-t 1] [-r 0|1|2] [-i graph.gfa] [-V 0]
 //
 // Reads FASTA/FASTQ, optionally gzip-compressed (src/handle_input.cpp:13-43).
-// -r 0 prints the consensus, -r 1 the row-column MSA, -r 2 the graph as GFA. Exit codes follow the
+// -r 0 prints the consensus, -r 1 the row-column MSA, -r 2 the graph as GFA;
+// -i extends the graph of a GFA file (its paths count as reads). Exit codes follow the
 // reference: a backtrack that leaves the band exits 0 with no output
 // (src/align.cpp:1584-1588), a backtrack error exits 1 (src/align.cpp:1730).
 #include <zlib.h>
@@ -82,6 +83,8 @@ void usage() {
                  "  -f, --band_f INT       band f [40]\n"
                  "  -B, --ab_band          adaptive band\n"
                  "  -S, --seeding          minimizer seeding and anchoring\n"
+                 "  -p, --progressive_poa  progressive read order (guide tree)\n"
+                 "  -i, --inc_fp FILE      extend the graph of a GFA file\n"
                  "  -k, --k_mer INT        k-mer length [19]\n"
                  "  -w, --mm_w INT         minimizer window [10]\n"
                  "  -W, --poa_w INT        minimum distance between anchors [unset]\n"
@@ -96,7 +99,7 @@ void usage() {
 int main(int argc, char** argv) {
     poa_params p;
     poa_params_init(&p);
-    std::string path;
+    std::string path, inc_fp;
     int32_t sample_num = 50;  // -s: parsed and unused, as in the reference (src/main.cpp:69-70)
     struct Opt {
         char s;
@@ -116,6 +119,13 @@ int main(int argc, char** argv) {
         std::string o = argv[a];
         if (o == "-h" || o == "--help") { usage(); return 0; }
         if (o.size() < 2 || o[0] != '-') { path = o; continue; }
+        if (o == "-i" || o == "--inc_fp") {
+            if (a + 1 >= argc) { std::cerr << "error parsing options: missing value for " << o << "\n"; return 1; }
+            inc_fp = argv[++a];
+            continue;
+        }
+        if (o.compare(0, 9, "--inc_fp=") == 0) { inc_fp = o.substr(9); continue; }
+        if (o.compare(0, 2, "-i") == 0 && o.size() > 2) { inc_fp = o.substr(2); continue; }
         bool done = false;
         for (const Flag& f : flags)
             if (o == std::string("-") + f.s || o == std::string("--") + f.l) { *f.v = 1; done = true; }
@@ -161,7 +171,16 @@ int main(int argc, char** argv) {
     }
     char* text = nullptr;
     size_t tl = 0;
-    int st = poa_run(ctx, (int32_t)recs.size(), seqs.data(), lens.data(), hdrs.data(), &text, &tl, nullptr);
+    int st;
+    if (!inc_fp.empty()) {
+        // an unreadable graph file leaves the graph empty, as read_gfa does (src/handle_input.cpp:453-455)
+        std::string gfa;
+        if (!read_all(inc_fp.c_str(), gfa)) gfa.clear();
+        st = poa_run_gfa(ctx, gfa.data(), gfa.size(), (int32_t)recs.size(), seqs.data(), lens.data(), hdrs.data(),
+                         &text, &tl, nullptr);
+    } else {
+        st = poa_run(ctx, (int32_t)recs.size(), seqs.data(), lens.data(), hdrs.data(), &text, &tl, nullptr);
+    }
     if (st == POA_BAND_ESCAPE) { poa_destroy(ctx); return 0; }
     if (st == POA_BT_FAIL) { std::cerr << " backtrack error" << "\n"; poa_destroy(ctx); return 1; }
     if (st != POA_OK) {

@@ -9,7 +9,9 @@ reference's own sources into ``oracle/_ref/``):
 For every case it writes ``<case>.fa`` (seeded synthetic input),
 ``<case>.out`` (the reference CLI's stdout, byte for byte: consensus, MSA or GFA) and, where the case
 has per-call records, ``<case>.dump`` (one score + path per alignment() call,
-from ``oracle/ref_harness``). ``manifest.json`` lists the cases and options.
+from ``oracle/ref_harness``). ``manifest.json`` lists the cases and options; an ``-i`` case names its graph
+file ``<case>.gfa`` (relative to this directory), the reference's own GFA
+output on seeded base reads.
 The fixtures are kept small so the CPU test-suite stays fast; the full-size
 configurations are checked on the GPU through size-independent properties and
 against the CPU restatement.
@@ -87,6 +89,23 @@ def cases():
     return out
 
 
+def inc_cases():
+    """-i cases: (name, reads to add, options, reads the graph is made of). The
+    graph file <name>.gfa is the reference's own -r 2 output on the base reads.
+    Not covered: -i with -S or -p (the reference aborts) and with -r 2 (it
+    writes the GFA paths out of bounds)."""
+    fam = synth.single_graph_msa(seed=19, nseq=12, length=600)
+    noisy = synth.noisy_long_reads(seed=29, nreads=6, length=900)
+    names = [f"g{i}" for i in range(12)]
+    return [
+        ("inc_cons", fam[8:], [], (fam[:8], names[:8])),
+        ("inc_msa", fam[8:], ["-r", "1"], (fam[:8], names[:8])),
+        ("inc_adaptive", noisy[3:], ["-B"], (noisy[:3], names[:3])),
+        ("inc_graph_only", [], [], (fam[:5], names[:5])),
+        ("inc_graph_only_msa", [], ["-r", "1"], (fam[:5], names[:5])),
+    ]
+
+
 # Full-size configurations: inputs are regenerated from their seeds by the
 # tests; only the md5 of the reference's stdout is stored.
 FULLSIZE = [
@@ -123,6 +142,21 @@ def main():
         fullsize()
         return
     manifest = []
+    for name, reads, opts, (base, base_names) in inc_cases():
+        bfa = os.path.join("/tmp", name + "_base.fa")
+        synth.write_fasta(bfa, base, base_names)
+        gfa = subprocess.run([REF_BIN, bfa, "-r", "2"], capture_output=True, check=True).stdout
+        os.unlink(bfa)
+        with open(os.path.join(HERE, name + ".gfa"), "wb") as fh:
+            fh.write(gfa)
+        fa = os.path.join(HERE, name + ".fa")
+        synth.write_fasta(fa, reads)
+        full = ["-i", name + ".gfa"] + opts
+        res = subprocess.run([REF_BIN, fa, "-i", os.path.join(HERE, name + ".gfa")] + opts, capture_output=True,
+                             check=True)
+        with open(os.path.join(HERE, name + ".out"), "wb") as fh:
+            fh.write(res.stdout)
+        manifest.append({"case": name, "opts": full, "nseq": len(reads), "dump": False})
     for name, reads, opts, dump in cases():
         fa = os.path.join(HERE, name + ".fa")
         synth.write_fasta(fa, reads)

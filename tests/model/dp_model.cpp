@@ -205,8 +205,17 @@ extern "C" {
 
 // Run the whole driver with the model engine. params: match, mismatch,
 // gap_open, gap_ext, b, f, ab_band, result, seeding. Returns status; *text is malloc'd.
+int model_run_gfa(int nseq, const char* const* seqs, const int* lens, const int* params, const char* gfa,
+                  int gfa_len, const char* const* hdrs, char** text, int* scores, int scores_cap);
+
 int model_run(int nseq, const char* const* seqs, const int* lens, const int* params, char** text,
               int* scores, int scores_cap) {
+    return model_run_gfa(nseq, seqs, lens, params, nullptr, -1, nullptr, text, scores, scores_cap);
+}
+
+// gfa_len < 0: no graph file (plain run); hdrs may be null
+int model_run_gfa(int nseq, const char* const* seqs, const int* lens, const int* params, const char* gfa,
+                  int gfa_len, const char* const* hdrs, char** text, int* scores, int scores_cap) {
     Params p;
     p.match = params[0]; p.mismatch = params[1]; p.gap_open1 = params[2]; p.gap_ext1 = params[3];
     p.b = params[4]; p.f = params[5]; p.ab_band = params[6]; p.result = params[7]; p.enable_seeding = params[8];
@@ -214,10 +223,14 @@ int model_run(int nseq, const char* const* seqs, const int* lens, const int* par
     normalize_params(p);
     std::vector<std::string> s(nseq), headers;
     for (int i = 0; i < nseq; i++) s[i].assign(seqs[i], lens[i]);
+    if (hdrs)
+        for (int i = 0; i < nseq; i++) headers.push_back(hdrs[i] ? hdrs[i] : "");
     ModelEngine eng;
     std::string out;
     std::vector<int32_t> sc;
-    int st = run_reads(p, s, headers, eng, out, &sc, nullptr);
+    std::string g;
+    if (gfa_len >= 0) g.assign(gfa ? gfa : "", (size_t)gfa_len);
+    int st = run_reads(p, s, headers, eng, out, &sc, nullptr, gfa_len >= 0 ? &g : nullptr);
     *text = (char*)malloc(out.size() + 1);
     memcpy(*text, out.data(), out.size());
     (*text)[out.size()] = 0;

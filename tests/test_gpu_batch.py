@@ -64,6 +64,16 @@ def test_batch_golden_edges():
     _check(["edge_mixed", "edge_single", "edge_empty_read", "edge_all_n", "edge_identical", "cons_small"], [])
 
 
+def test_batch_golden_fullband():
+    # f = 0: every row spans the whole query (the dynamic-band fill without the adaptive update)
+    _check(["cons_fullband"], ["-f", "0"])
+
+
+def test_batch_golden_edges_adaptive():
+    _check(["edge_mixed_adaptive", "edge_single_adaptive", "edge_empty_read_adaptive", "edge_all_n_adaptive",
+            "edge_identical_adaptive"], ["-B"])
+
+
 def test_batch_golden_scoring():
     _check(["cons_scoring"], MANIFEST["cons_scoring"]["opts"])
 

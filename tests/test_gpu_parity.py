@@ -18,7 +18,7 @@ from tests import fasta
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = os.path.join(HERE, "golden")
 with open(os.path.join(GOLD, "manifest.json")) as fh:
-    CASES = [c for c in json.load(fh) if "-S" not in c["opts"] and "-p" not in c["opts"]]
+    CASES = json.load(fh)
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +29,11 @@ def test_golden(case):
     _, seqs = fasta.read(fa)
     params = poa_b200.Params.from_cli(case["opts"])
     with poa_b200.Context(params) as ctx:
-        text, scores = ctx.run(seqs, fasta.headers(fa))
+        if "-i" in case["opts"]:
+            with open(os.path.join(GOLD, case["opts"][case["opts"].index("-i") + 1]), "rb") as fh:
+                text, scores = ctx.run_gfa(fh.read(), seqs, fasta.headers(fa))
+        else:
+            text, scores = ctx.run(seqs, fasta.headers(fa))
     with open(os.path.join(GOLD, case["case"] + ".out"), "rb") as fh:
         assert text == fh.read()
     if case["dump"]:
@@ -67,7 +71,8 @@ def test_seeded_vs_oracle(name, gen, opts, oracle_bin, tmp_path):
 
 
 CLI = os.path.join(os.path.dirname(HERE), "poa_b200", "minipoa_b200")
-CLI_CASES = ["cons_small", "msa_small", "noisy_adaptive", "cons_scoring", "edge_mixed_msa", "window_00"]
+CLI_CASES = ["cons_small", "msa_small", "noisy_adaptive", "cons_scoring", "edge_mixed_msa", "window_00",
+             "gfa_small", "edge_empty_read_gfa", "prog_msa", "seeded_msa", "inc_msa", "inc_adaptive"]
 
 
 @pytest.mark.parametrize("name", CLI_CASES)
@@ -75,7 +80,8 @@ def test_cli_drop_in(name):
     """minipoa_b200 prints exactly what minipoa prints, given the same options."""
     case = [c for c in CASES if c["case"] == name][0]
     fa = os.path.join(GOLD, name + ".fa")
-    res = subprocess.run([CLI, fa] + case["opts"], capture_output=True, timeout=120)
+    opts = [os.path.join(GOLD, o) if k > 0 and case["opts"][k - 1] == "-i" else o for k, o in enumerate(case["opts"])]
+    res = subprocess.run([CLI, fa] + opts, capture_output=True, timeout=120)
     assert res.returncode == 0, res.stderr
     with open(os.path.join(GOLD, name + ".out"), "rb") as fh:
         assert res.stdout == fh.read()

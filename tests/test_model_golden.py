@@ -38,6 +38,11 @@ def model():
     lib.model_run.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int),
                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_void_p),
                               ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.model_run_gfa.restype = ctypes.c_int
+    lib.model_run_gfa.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_void_p),
+                                  ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.model_free.argtypes = [ctypes.c_void_p]
     return lib
 
@@ -47,7 +52,9 @@ def opts_to_params(opts):
     it = iter(opts)
     for o in it:
         k = o.lstrip("-")
-        if k in ("B", "S", "p"):
+        if k == "i":
+            next(it)
+        elif k in ("B", "S", "p"):
             p[k] = 1
         else:
             p[k] = int(next(it))
@@ -58,12 +65,19 @@ def opts_to_params(opts):
 def test_model_matches_reference(case, model):
     names, seqs = fasta.read(os.path.join(GOLD, case["case"] + ".fa"))
     n = len(seqs)
-    arr = (ctypes.c_char_p * n)(*seqs)
-    lens = (ctypes.c_int * n)(*[len(s) for s in seqs])
+    arr = (ctypes.c_char_p * max(n, 1))(*seqs)
+    lens = (ctypes.c_int * max(n, 1))(*[len(s) for s in seqs])
     par = (ctypes.c_int * 10)(*opts_to_params(case["opts"]))
     out = ctypes.c_void_p()
     scores = (ctypes.c_int * (n + 1))()
-    st = model.model_run(n, arr, lens, par, ctypes.byref(out), scores, n + 1)
+    if "-i" in case["opts"]:
+        with open(os.path.join(GOLD, case["opts"][case["opts"].index("-i") + 1]), "rb") as fh:
+            g = fh.read()
+        hdr = fasta.headers(os.path.join(GOLD, case["case"] + ".fa"))
+        harr = (ctypes.c_char_p * max(n, 1))(*[h.encode() for h in hdr])
+        st = model.model_run_gfa(n, arr, lens, par, g, len(g), harr, ctypes.byref(out), scores, n + 1)
+    else:
+        st = model.model_run(n, arr, lens, par, ctypes.byref(out), scores, n + 1)
     text = ctypes.string_at(out.value)
     model.model_free(out)
     assert st == 0

@@ -14,10 +14,10 @@ import pytest
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 with open(os.path.join(GOLD, "manifest.json")) as fh:
     MANIFEST = json.load(fh)
-# seeding (-S) and the progressive order (-p) are host-side minimizer steps the
+# seeding (-S), the progressive order (-p) and GFA input (-i) are host-side steps the
 # restatement leaves out; the product's host driver is checked on them through
 # the CPU model of the kernels (test_model_golden.py) and on the GPU
-CASES = [c for c in MANIFEST if "-S" not in c["opts"] and "-p" not in c["opts"]]
+CASES = [c for c in MANIFEST if not {"-S", "-p", "-i"} & set(c["opts"])]
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])

@@ -1060,6 +1060,76 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
 // (src/align.cpp:1516-1568). out[4] / out[5]: record bytes and spilled
 // row-store entries used.
 constexpr int DYN_STAGE_EDGES = 128;
+// prefetched adaptive-update inputs (int32 slots): predecessors' Sl, Mp; successors'
+// Ol, Or, Pl, Pr, Ow and row index; the row's own Sl, Ow, Ol, Or
+constexpr int UPD_PSL = 0, UPD_PMP = 32, UPD_SOL = 64, UPD_SOR = 96, UPD_SPL = 128, UPD_SPR = 160, UPD_SOW = 192,
+              UPD_SROW = 224, UPD_OWN = 256, UPD_INTS = 260, UPD_BYTES = 1088;
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_all() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// adaptive_update_warp with its inputs already in shared memory (copied with
+// cp.async when the row started; nothing else writes them in between: the
+// predecessors are finished, and only this row's update changes its own and
+// its successors' state). Needs d <= 32 predecessors and ns <= 32 successors.
+__device__ void adaptive_update_pf(const DpArgs& a, int i, int Bs, int max_j, int lane, const int32_t* upd, int d,
+                                   int ns, int base_i, int hql, const uint8_t* __restrict__ qf) {
+    const int n = a.v.n;
+    int32_t* Mp = a.state + AB_MP * n;
+    int32_t* Sl = a.state + AB_SL * n;
+    int32_t* Pl = a.state + AB_PL * n;
+    int32_t* Pr = a.state + AB_PR * n;
+    int32_t* Ol = a.state + AB_OL * n;
+    int32_t* Or = a.state + AB_OR * n;
+    int32_t* Ow = a.state + AB_OW * n;
+    const int max_acj = Bs * BLK + max_j;
+    const bool base_match = base_i == (int)qf[max_acj + 1];  // cur.base == seq[max_acj]
+    int sl_best = INT_MIN, max_slp = 0;
+    bool is_match = false;
+    if (base_match) {
+        if (lane < d) {
+            const int slp = upd[UPD_PSL + lane];
+            max_slp = slp;
+            if (upd[UPD_PMP + lane] + 1 == max_acj) {
+                is_match = true;
+                sl_best = slp + 1;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
+            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
+        }
+        is_match = __any_sync(0xffffffffu, is_match);
+    }
+    int sl_i = upd[UPD_OWN + 0], ow_i = upd[UPD_OWN + 1], ol_i = upd[UPD_OWN + 2], or_i = upd[UPD_OWN + 3];
+    if (is_match) sl_i = mx(sl_i, sl_best);
+    if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
+    if (sl_i >= 30) {
+        ol_i = or_i = max_acj - hql;
+        ow_i = 0;
+    }
+    if (lane == 0) {
+        Mp[i] = max_acj;
+        Sl[i] = sl_i;
+        Ow[i] = ow_i;
+        Ol[i] = ol_i;
+        Or[i] = or_i;
+    }
+    if (lane < ns) {
+        const int s = upd[UPD_SROW + lane];
+        Ol[s] = sl_i >= 30 ? ol_i : mn(upd[UPD_SOL + lane], ol_i);
+        Or[s] = sl_i >= 30 ? or_i : mx(upd[UPD_SOR + lane], or_i);
+        Pl[s] = mn(upd[UPD_SPL + lane], max_acj);
+        Pr[s] = mx(upd[UPD_SPR + lane], max_acj + 1);
+        Ow[s] = ow_i ? mx(upd[UPD_SOW + lane], ow_i) : ow_i;
+    }
+    __syncwarp();
+}
 
 // adaptive_update (dp_rowops.h, src/align.cpp:1516-1568) with the warp: the
 // predecessors' slope test and the successors' band updates run one lane per
@@ -1136,7 +1206,7 @@ __device__ void adaptive_update_warp(const DpArgs& a, int i, int Bs, int max_j, 
 }
 
 __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const int32_t* __restrict__ vmaxs,
-                                 const uint8_t* __restrict__ qsm, int4* sed, int lane) {
+                                 const uint8_t* __restrict__ qsm, int4* sed, int32_t* upd, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
     const bool adaptive = a.f > 0 && a.ab_band;
     if (adaptive)
@@ -1171,15 +1241,46 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
             rm.Bs = Bs; rm.Be = Be; rm.st = row_st; rm.tb = tb_next;
             a.meta[i] = rm;
         }
+        // the adaptive update's inputs, copied while the row is filled
+        int ns = 0, base_i = 0, hql = 0;
+        bool pf = false;
+        if (adaptive && i >= 1) {
+            const int o0 = a.v.out_ptr[i];
+            ns = a.v.out_ptr[i + 1] - o0;
+            base_i = a.v.base[i];
+            hql = a.v.hq_loc[i];
+            pf = d <= 32 && ns <= 32;
+            if (pf) {
+                const int32_t* st_ = a.state;
+                if (lane < ns) {
+                    const int sr = a.v.out_row[o0 + lane];
+                    upd[UPD_SROW + lane] = sr;
+                    cp_async4(upd + UPD_SOL + lane, st_ + AB_OL * n + sr);
+                    cp_async4(upd + UPD_SOR + lane, st_ + AB_OR * n + sr);
+                    cp_async4(upd + UPD_SPL + lane, st_ + AB_PL * n + sr);
+                    cp_async4(upd + UPD_SPR + lane, st_ + AB_PR * n + sr);
+                    cp_async4(upd + UPD_SOW + lane, st_ + AB_OW * n + sr);
+                }
+                if (lane < 4) {
+                    const int arr = lane == 0 ? AB_SL : lane == 1 ? AB_OW : lane == 2 ? AB_OL : AB_OR;
+                    cp_async4(upd + UPD_OWN + lane, st_ + arr * n + i);
+                }
+            }
+        }
         // predecessor records with the predecessors' bands and locations
         int4* er = d <= DYN_STAGE_EDGES ? sed : erec + e0;
         for (int k = lane; k < d; k += 32) {
             int4 rec = erec[e0 + k];
+            if (pf) {
+                cp_async4(upd + UPD_PSL + k, a.state + AB_SL * n + rec.x);
+                cp_async4(upd + UPD_PMP + k, a.state + AB_MP * n + rec.x);
+            }
             const RowMeta pm = a.meta[rec.x];
             rec.x = pm.Bs | (pm.Be << 16);
             rec.y = (int32_t)pm.st;
             er[k] = rec;
         }
+        if (pf) cp_async_commit_all();
         __syncwarp();
         RowDesc cur;
         cur.bsbe = Bs | (Be << 16);
@@ -1208,7 +1309,13 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
                                            (unsigned long long)(0xffffffffu - (uint32_t)bestJ);
             key = warp_max_u64(key);
             const int max_j = bn > 0 ? (int)(0xffffffffu - (uint32_t)(key & 0xffffffffu)) : 0;
-            adaptive_update_warp(a, i, Bs, max_j, lane);
+            if (pf) {
+                cp_async_wait_all();
+                __syncwarp();
+                adaptive_update_pf(a, i, Bs, max_j, lane, upd, d, ns, base_i, hql, qsm);
+            } else {
+                adaptive_update_warp(a, i, Bs, max_j, lane);
+            }
         }
         tb_next = (tb_next + (int64_t)bn * BLK * bpc + 15) & ~(int64_t)15;
         __syncwarp();
@@ -1518,18 +1625,19 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
             dp_fill_warp_static(a, (const RowDesc*)(s + L.v_desc), (const int4*)(s + L.v_pmeta), (int32_t*)wsm,
                                 A.sring_blocks, qsm, stage, lane);
         } else {
-            // shared memory: staged records, and the query when it fits
+            // shared memory: staged records, the update's inputs, and the query when it fits
             const uint8_t* qf = qs;
             int4* sed = reinterpret_cast<int4*>(wsm);
             const int64_t sed_bytes = (int64_t)DYN_STAGE_EDGES * 16;
-            if (sed_bytes + qsb <= A.smem_per_warp) {
-                uint8_t* qsm = wsm + sed_bytes;
+            int32_t* upd = reinterpret_cast<int32_t*>(wsm + sed_bytes);
+            if (sed_bytes + UPD_BYTES + qsb <= A.smem_per_warp) {
+                uint8_t* qsm = wsm + sed_bytes + UPD_BYTES;
                 for (int64_t x = lane * 16; x < qsb; x += 32 * 16)
                     *reinterpret_cast<uint4*>(qsm + x) = *reinterpret_cast<const uint4*>(qs + x);
                 qf = qsm;
             }
             __syncwarp();
-            dp_fill_warp_dyn(a, (int4*)(s + L.v_pmeta), (const int32_t*)(s + L.v_desc), qf, sed, lane);
+            dp_fill_warp_dyn(a, (int4*)(s + L.v_pmeta), (const int32_t*)(s + L.v_desc), qf, sed, upd, lane);
         }
         __syncwarp();
         {
@@ -1867,7 +1975,7 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     if (sring_rows < 2) sring_rows = 0;
     if (p_.f > 0 && !p_.ab_band && qsm_bytes + stage_bytes > smem_w)
         throw std::invalid_argument("reads too long for the batch kernel's shared memory; raise smem_per_warp");
-    if (!(p_.f > 0 && !p_.ab_band) && smem_w < DYN_STAGE_EDGES * 16)
+    if (!(p_.f > 0 && !p_.ab_band) && smem_w < DYN_STAGE_EDGES * 16 + UPD_BYTES)
         throw std::invalid_argument("smem_per_warp too small for the adaptive-band fill");
     if (smem_w % 16 != 0) throw std::invalid_argument("smem_per_warp must be a multiple of 16");
     int occ = 0;

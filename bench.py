@@ -349,15 +349,18 @@ def ours(args, world, rank, local, D):
     kernel_s = D.max(sum(kern_ms) / 1e3) / args.steps
     peaks = load_peaks()
     achieved = cells * BYTES_PER_CELL / kernel_s / 1e9
+    int_ops = cells * OPS_PER_CELL + st["edge_cells"] * OPS_PER_EDGE_CELL + (cells if wl["opts"] == ["-B"] else 0)
     tpc = profile_traffic_per_cell(args.workload)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_src": peaks["src"],
                 "traffic": (tpc * cells if tpc is not None else None),
                 "algorithmic_bytes_per_launch": cells * BYTES_PER_CELL, "kernel": "k_batch",
                 "kernel_s_per_step": kernel_s,
-                "int_ops_frac": (cells * OPS_PER_CELL / kernel_s) / int_peak_ops(clocks.get("sm_mhz")),
-                "int_ops_note": "lower bound: 5 int32 ops per cell (edge-cell ops not counted), "
-                                "nominal peak 148 SMs x 128 lanes x median SM clock"}
+                "int_ops_frac": int_ops / kernel_s / int_peak_ops(clocks.get("sm_mhz")),
+                "int_ops_per_launch": int_ops,
+                "int_ops_note": "5 int32 ops per cell + 7 per edge-cell (cell x in-window predecessor)"
+                                + (" + 1 per cell for the adaptive argmax" if wl["opts"] == ["-B"] else "")
+                                + "; nominal int32 peak 148 SMs x 128 lanes x median SM clock"}
     line = {
         "metric": METRIC, "value": value, "unit": "windows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
@@ -418,21 +421,30 @@ def reference(args, world, rank, local, D):
     kind = "reference" if binary == REF_BIN else "port"
     cores = len(os.sched_getaffinity(0))
     per_step = min(args.windows or wl["windows"], wl["ref_windows_per_core"] * cores)
-    ws = make_windows(wl, 0, per_step)
+    # every step (warm-up ones too) takes the next windows of the seeded set, so the
+    # timed steps see windows of every size rather than the same few again
+    total = min(args.windows or wl["windows"], per_step * (args.warmup + args.steps))
+    ws = make_windows(wl, 0, total)
+    chunk = lambda k: range((k * per_step) % total, min((k * per_step) % total + per_step, total))
     with tempfile.TemporaryDirectory() as d:
-        paths = write_windows(ws, range(per_step), d)
-        for _ in range(args.warmup):
-            run_cpu_windows(binary, paths[:cores], cores, wl["opts"])
+        paths = write_windows(ws, range(total), d)
+        for k in range(args.warmup):
+            run_cpu_windows(binary, [paths[w] for w in chunk(k)], cores, wl["opts"])
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            run_cpu_windows(binary, paths, cores, wl["opts"])
+        done = 0
+        for k in range(args.warmup, args.warmup + args.steps):
+            idx = chunk(k)
+            run_cpu_windows(binary, [paths[w] for w in idx], cores, wl["opts"])
+            done += len(idx)
         dt = time.perf_counter() - t0
-    v = per_step * args.steps / dt
+    per_step = done / max(args.steps, 1)
+    v = done / dt
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "windows/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": wl["desc"], "windows_per_step": per_step, "mode": wl["mode"]},
+            "config": {"workload": wl["desc"], "windows_per_step": per_step, "mode": wl["mode"],
+                       "sample": f"{done} windows in {args.steps} steps, the next {per_step:.0f} of the seeded set each"},
             "cpu_baseline": {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
                              "sample": f"{per_step} windows per step, one {kind} process per window "
                                        f"({' '.join(wl['opts']) or 'default options'}), {cores} concurrent"},

@@ -148,8 +148,9 @@ int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, con
  * and were re-run with the default sizing, [15] device time of the batch
  * kernel launches of the last run in microseconds, [16] device time of the
  * whole last run (plan, launches, re-runs) in microseconds, [17] device time
- * of the proposer's plan in microseconds (0 without a proposer). */
-int poa_batch_stats(poa_ctx* ctx, int64_t* out18);
+ * of the proposer's plan in microseconds (0 without a proposer), [18] edge
+ * cells of the last run (band cells x in-window predecessors of their row). */
+int poa_batch_stats(poa_ctx* ctx, int64_t* out19);
 /* Resource plan for the uploaded windows (no counterpart in the reference:
  * the reference allocates per alignment). One value per window: graph nodes,
  * traceback record bytes and spilled row-store entries (int32) of its

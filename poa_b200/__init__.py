@@ -302,12 +302,12 @@ class Context:
                 self._check(lib().poa_batch_config(self._h, key, int(val)))
 
     def batch_stats(self) -> dict:
-        o = (ctypes.c_int64 * 18)()
+        o = (ctypes.c_int64 * 19)()
         self._check(lib().poa_batch_stats(self._h, o))
         names = ("view", "fill", "backtrack", "fusion", "topsort", "consensus")
         return dict(cells=o[0], failed=o[1], slots=o[2], slot_bytes=o[3], h2d_bytes=o[4], d2h_bytes=o[5],
                     phase_cycles={names[k]: o[6 + k] for k in range(6)}, launches=o[12], retried=o[13],
-                    fallback=o[14], kernel_us=o[15], run_us=o[16], plan_us=o[17])
+                    fallback=o[14], kernel_us=o[15], run_us=o[16], plan_us=o[17], edge_cells=o[18])
 
     def batch_plan(self, nodes=None, tb_bytes=None, spill=None, cost=None):
         """Per-window resource plan (see poa_batch_plan); no arguments clears it."""

@@ -95,7 +95,7 @@ struct BatchArgs {
     int32_t cons_stride;
     int32_t* cons_len;
     int32_t* status;
-    int64_t* cells;
+    int64_t* cells;  // [n_windows * 2] band cells and edge-cells (cells x in-window predecessors)
     int64_t* phase;  // [n_windows * NPHASE] lane-0 clock cycles per phase
     int32_t* rstats; // [n_reads * NRSTAT] per read, see BatchEngine::read_stats
 };
@@ -1011,7 +1011,7 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
     const int32_t K = add32(add32(NEG_INF, sc.e1), -sc.o1);
     RowDesc* sdesc = reinterpret_cast<RowDesc*>(stage);
     int4* serec = reinterpret_cast<int4*>(stage + STAGE_ROWS * sizeof(RowDesc));
-    int64_t cells = 0;
+    int64_t cells = 0, ecells = 0;
     for (int i0 = 0; i0 < n; i0 += STAGE_ROWS) {
         const int cnt = min(STAGE_ROWS, n - i0);
         // stage: descriptors of rows i0.., and their predecessor records when they fit
@@ -1030,7 +1030,9 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         const int4* er_base = staged ? serec - e_lo : erec;
         for (int i = i0; i < i0 + cnt; i++) {
             const RowDesc cur = sdesc[i - i0];
-            cells += (int64_t)((cur.bsbe >> 16) - (cur.bsbe & 0xffff) - 1) * BLK;
+            const int64_t rc = (int64_t)((cur.bsbe >> 16) - (cur.bsbe & 0xffff) - 1) * BLK;
+            cells += rc;
+            ecells += rc * cur.d;
             int32_t bm = 0;
             int bj = 0;
             fill_row<false>(a, cur, er_base, ring, RB, qsm, i, lane, bm, bj);
@@ -1043,6 +1045,7 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
         const int32_t* src = blk_src(ring, a.rs, RB, (int)last.st);
         a.out[1] = src[(jm / BLK) * 16 + jm % BLK];
         a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+        a.out[6] = (int32_t)(ecells > INT_MAX ? INT_MAX : ecells);
         a.out[0] = ST_OK;
     }
     __syncwarp();
@@ -1213,7 +1216,7 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
         for (int r = lane; r < n; r += 32) adaptive_init_entry(a, r, m);
     __syncwarp();
     const int64_t ring_part = (int64_t)a.ring_rows * a.ring_blocks * 16;
-    int64_t st_next = ring_part, tb_next = 0, cells = 0;
+    int64_t st_next = ring_part, tb_next = 0, cells = 0, ecells = 0;
     for (int i = 0; i < n; i++) {
         int Bs, Be;
         row_band(a, i, m, Bs, Be);
@@ -1302,6 +1305,7 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
         if (adaptive) fill_row<true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
         else fill_row<false>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
         cells += (int64_t)bn * BLK;
+        ecells += (int64_t)bn * BLK * d;
         if (adaptive && i >= 1) {
             // first maximum of the row: largest M, then smallest column
             unsigned long long key = bestM == INT_MIN ? 0ull
@@ -1325,6 +1329,7 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
         const int jm = m - last.Bs * BLK;
         a.out[1] = a.rs[last.st + (int64_t)(jm / BLK) * 16 + jm % BLK];
         a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+        a.out[6] = (int32_t)(ecells > INT_MAX ? INT_MAX : ecells);
         a.out[4] = (int32_t)tb_next;
         a.out[5] = (int32_t)(st_next - ring_part);
         a.out[0] = ST_OK;
@@ -1532,7 +1537,7 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
     const bool lens = A.f > 0;
     constexpr bool static_band = STATIC;  // f > 0 && !ab_band (checked on the host)
     int status = ST_OK;
-    int64_t cells = 0;
+    int64_t cells = 0, ecells = 0;
     long long ph[NPHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long tc = clock64();
     auto tick = [&](int k) {
@@ -1673,6 +1678,7 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
                                     a.moves, a.moves_cap, nm, lane);
             if (lane == 0) {
                 cells += a.out[3];
+                ecells += a.out[6];
                 g.hdr[2] = st;
                 g.hdr[13] = nm;
                 g.hdr[12] = g.hdr[12] + 1;  // fusion stamp, increasing over the slot's lifetime
@@ -1680,6 +1686,7 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         } else if (lane == 0) {
             int st = a.out[0];
             cells += a.out[3];
+            ecells += a.out[6];
             int32_t nm = 0;
             if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
             g.hdr[2] = st;
@@ -1722,7 +1729,8 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         tick(PH_CONS);
         A.cons_len[w] = len < 0 ? 0 : len;
         A.status[w] = status;
-        A.cells[w] = cells;
+        A.cells[2 * (int64_t)w] = cells;
+        A.cells[2 * (int64_t)w + 1] = ecells;
         for (int k = 0; k < NPHASE; k++) A.phase[(int64_t)w * NPHASE + k] = ph[k];
     }
     __syncwarp();
@@ -1828,7 +1836,7 @@ void BatchEngine::upload(const BatchInput& in, const Params& p) {
     o = up256((size_t)n_windows_ * cons_stride_);
     out_len_ = o; o = up256(o + 4 * (size_t)n_windows_);
     out_status_ = o; o = up256(o + 4 * (size_t)n_windows_);
-    out_cells_ = o; o = up256(o + 8 * (size_t)n_windows_);
+    out_cells_ = o; o = up256(o + 16 * (size_t)n_windows_);
     out_phase_ = o; o = up256(o + 8 * (size_t)NPHASE * n_windows_);
     out_rstats_ = o; o = up256(o + 4 * (size_t)NRSTAT * n_reads_);
     out_bytes_ = o;
@@ -2072,10 +2080,12 @@ void BatchEngine::sync_stats() {
     const int64_t* cl = (const int64_t*)(h + out_cells_);
     const int64_t* ph = (const int64_t*)(h + out_phase_);
     stats.cells = 0;
+    stats.edge_cells = 0;
     stats.failed = 0;
     for (int k = 0; k < 8; k++) stats.phase_cycles[k] = 0;
     for (int w = 0; w < n_windows_; w++) {
-        stats.cells += cl[w];
+        stats.cells += cl[2 * (int64_t)w];
+        stats.edge_cells += cl[2 * (int64_t)w + 1];
         stats.failed += st[w] != ST_OK;
         for (int k = 0; k < NPHASE; k++) stats.phase_cycles[k] += ph[(int64_t)w * NPHASE + k];
     }
@@ -2093,11 +2103,13 @@ void BatchEngine::download(std::vector<std::string>& cons, std::vector<int32_t>&
     cons.resize(n_windows_);
     status.resize(n_windows_);
     stats.cells = 0;
+    stats.edge_cells = 0;
     stats.failed = 0;
     for (int w = 0; w < n_windows_; w++) {
         cons[w].assign(h + out_cons_ + (size_t)w * cons_stride_, (size_t)ln[w]);
         status[w] = st[w];
-        stats.cells += cl[w];
+        stats.cells += cl[2 * (int64_t)w];
+        stats.edge_cells += cl[2 * (int64_t)w + 1];
         stats.failed += st[w] != ST_OK;
     }
 }

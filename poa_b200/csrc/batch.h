@@ -44,6 +44,7 @@ struct BatchStats {
     double run_ms = 0.0;      // device time of the whole last run(): plan, launches, re-runs
     double plan_ms = 0.0;     // device time of the proposer's plan inside run()
     int64_t cells = 0;        // DP band cells of the last run
+    int64_t edge_cells = 0;   // band cells x in-window predecessors of their rows
     int64_t dp_calls = 0;
     int32_t slots = 0;        // concurrent windows (warps) of the persistent launch
     int64_t slot_bytes = 0;

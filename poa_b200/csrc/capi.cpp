@@ -343,6 +343,7 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* o) {
     o[15] = (int64_t)(s.kernel_ms * 1000.0);
     o[16] = (int64_t)(s.run_ms * 1000.0);
     o[17] = (int64_t)(s.plan_ms * 1000.0);
+    o[18] = s.edge_cells;
     return POA_OK;
 }
 

@@ -280,12 +280,20 @@ def ours(args, world, rank, local, D):
     if wl["proposer"] and not args.no_proposer:
         prop = poa_b200.Proposer(device=local, weights=poa_b200.PROP_WEIGHTS)
         ctx.batch_use_proposer(prop)
+    shape = {"source": "engine defaults"}
+    if not (args.blocks_per_sm or args.smem_per_warp or args.no_autotuned):
+        t = ctx.batch_autotuned(args.workload)
+        if t:
+            shape = {"source": "poa_b200/tuned_launch.json (python -m poa_b200.autotune)",
+                     "blocks_per_sm": t["blocks_per_sm"], "smem_per_warp": t["smem_per_warp"]}
     if args.max_blocks:
         ctx.batch_config(max_blocks=args.max_blocks)
     if args.blocks_per_sm:
         ctx.batch_config(blocks_per_sm=args.blocks_per_sm)
+        shape = {"source": "command line", "blocks_per_sm": args.blocks_per_sm}
     if args.smem_per_warp:
         ctx.batch_config(smem_per_warp=args.smem_per_warp)
+        shape = dict(shape, source="command line", smem_per_warp=args.smem_per_warp)
 
     # ---- device-resident leg: plan + kernel(s) per step, device-timed
     ctx.batch_upload(ws)
@@ -376,7 +384,7 @@ def ours(args, world, rank, local, D):
         "gcups": world * cells * args.steps / t_dev / 1e9,
         "cells_per_step": cells, "failed_windows": failed,
         "gpu_launches": launches, "retried_windows": st["retried"], "e2e": e2e, "roofline": roofline, "clocks": clocks,
-        "slots": st["slots"], "slot_bytes": st["slot_bytes"],
+        "slots": st["slots"], "slot_bytes": st["slot_bytes"], "launch_shape": shape,
         "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
         "phase_mcycles_per_window": {k: v / 1e6 / ws.n_windows for k, v in st["phase_cycles"].items()},
     }
@@ -472,6 +480,7 @@ def main():
                     help="cap the persistent grid (small profiling captures); 0 = one full wave")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="batch kernel variant: 3 (default) or 4")
     ap.add_argument("--smem-per-warp", type=int, default=0, help="shared memory per warp in bytes")
+    ap.add_argument("--no-autotuned", action="store_true", help="ignore poa_b200/tuned_launch.json")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = WORKLOADS[args.workload]["steps"]

@@ -295,6 +295,14 @@ class Context:
         """Plan the uploaded windows' slots with the proposer (see poa_batch_propose)."""
         self._check(lib().poa_batch_propose(self._h, prop._h))
 
+    def batch_autotuned(self, workload: str) -> Optional[dict]:
+        """Apply the launch shape poa_b200.autotune recorded for ``workload`` (if any); returns it."""
+        from poa_b200 import autotune
+        t = autotune.load(workload)
+        if t:
+            self.batch_config(blocks_per_sm=t["blocks_per_sm"], smem_per_warp=t["smem_per_warp"])
+        return t
+
     def batch_config(self, blocks_per_sm=None, max_blocks=None, smem_per_warp=None):
         """Launch shape of the batch kernel (see poa_batch_config)."""
         for key, val in ((0, blocks_per_sm), (1, max_blocks), (2, smem_per_warp)):

@@ -45,6 +45,7 @@ struct SlotLayout {
 SlotLayout make_layout(int32_t NC, int32_t EC, int32_t QC, int32_t ring_rows, int32_t ring_blocks, int64_t spill,
                        int64_t tb_cap, bool adaptive) {
     SlotLayout L;
+    std::memset(&L, 0, sizeof L);
     L.NC = NC; L.EC = EC; L.QC = QC;
     L.ring_rows = ring_rows; L.ring_blocks = ring_blocks;
     L.rs_cap = (int64_t)ring_rows * ring_blocks * 16 + spill;
@@ -1778,6 +1779,7 @@ BatchEngine::~BatchEngine() {
     if (h_out_) cudaFreeHost(h_out_);
     for (void* e : {ev0_, ev1_, evr0_, evr1_, evp_})
         if (e) cudaEventDestroy((cudaEvent_t)e);
+    if (kgraph_exec_) cudaGraphExecDestroy((cudaGraphExec_t)kgraph_exec_);
     if (stream_) cudaStreamDestroy((cudaStream_t)stream_);
 }
 
@@ -1887,7 +1889,7 @@ void BatchEngine::run() {
             c.spill = std::max(c.spill, plan_spill_[w]);
         }
         c.NC = std::min<int64_t>(c.NC, 60000);
-        launch(plan_order_.data(), n_windows_, c);
+        launch(plan_order_.data(), n_windows_, c, PLAN_HEADROOM);
         first = 0;
     } else {
         launch(order_.data(), n_windows_, default_caps(1));
@@ -1959,7 +1961,7 @@ void BatchEngine::set_plan(const int32_t* nodes, const int64_t* tb_bytes, const 
     std::stable_sort(plan_order_.begin(), plan_order_.end(), [&](int a, int b) { return cost[a] > cost[b]; });
 }
 
-void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps) {
+void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps, double headroom) {
     cudaStream_t s = (cudaStream_t)stream_;
     int sms = 0;
     cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "attr");
@@ -1972,6 +1974,7 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     const int64_t tb_cap = (caps.tb_cap + 4095) / 4096 * 4096;
     const int64_t spill = (caps.spill + 63) / 64 * 64;
     SlotLayout L = make_layout(NC, EC, QC, ring_rows, ring_blocks, spill, tb_cap, adaptive);
+    const SlotLayout L_planned = L;
     const int warps = warps_per_block;
     const int smem_w = smem_per_warp;
     const size_t dyn = (size_t)warps * smem_w;
@@ -2006,6 +2009,19 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     size_t free_b = 0, total_b = 0;
     cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
     const size_t budget = (size_t)(0.75 * (double)(free_b + d_slots_cap_));
+    if (headroom > 1.0) {
+        // planned capacities: grow every slot by up to `headroom` while every resident
+        // warp still gets one, so a window a little beyond the plan still fits
+        const int want = std::max(1, std::min(blocks, (count + warps - 1) / warps));
+        const double fit = 0.97 * (double)budget / ((double)want * warps * (double)L_planned.bytes);
+        const double h = std::min(headroom, fit);
+        if (h > 1.0) {
+            const int32_t NCh = (int32_t)std::min<double>(60000.0, std::max(64.0, NC * h));
+            const int64_t tbh = ((int64_t)(tb_cap * h) + 4095) / 4096 * 4096;
+            const int64_t sph = ((int64_t)(spill * h) + 63) / 64 * 64;
+            L = make_layout(NCh, 3 * NCh, QC, ring_rows, ring_blocks, sph, tbh, adaptive);
+        }
+    }
     const int64_t max_by_mem = (int64_t)(budget / (size_t)L.bytes) / warps;
     if (max_by_mem < 1) throw std::runtime_error("not enough device memory for one batch slot");
     blocks = (int)std::min<int64_t>(blocks, max_by_mem);
@@ -2029,6 +2045,7 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     char* o = (char*)d_out_;
     cuda_check(cudaMemcpyAsync(d + off_order_, windows, 4 * (size_t)count, cudaMemcpyHostToDevice, s), "H2D order");
     BatchArgs A;
+    std::memset(&A, 0, sizeof A);  // padding too: the graph cache compares the bytes
     A.seq = (const uint8_t*)(d + off_seq_);
     A.read_off = (const int64_t*)(d + off_roff_);
     A.read_len = (const int32_t*)(d + off_rlen_);
@@ -2052,16 +2069,46 @@ void BatchEngine::launch(const int32_t* windows, int32_t count, const Caps& caps
     A.cells = (int64_t*)(o + out_cells_);
     A.phase = (int64_t*)(o + out_phase_);
     A.rstats = (int32_t*)(o + out_rstats_);
-    cuda_check(cudaMemsetAsync(A.counter, 0, 4, s), "memset counter");
-    cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
-    if (stat) {
-        if (dense) k_batch<4, true, 4><<<blocks, 4 * 32, dyn, s>>>(A);
-        else k_batch<4, true, 3><<<blocks, 4 * 32, dyn, s>>>(A);
-    } else {
-        if (dense) k_batch<4, false, 4><<<blocks, 4 * 32, dyn, s>>>(A);
-        else k_batch<4, false, 3><<<blocks, 4 * 32, dyn, s>>>(A);
+    // the work-counter reset and the persistent launch, recorded as a CUDA graph and
+    // replayed while the launch (variant, grid, shared memory, arguments) is unchanged
+    struct KKey {
+        bool stat, dense;
+        int blocks;
+        size_t dyn;
+        BatchArgs A;
+    } key;
+    std::memset(&key, 0, sizeof key);
+    key.stat = stat;
+    key.dense = dense;
+    key.blocks = blocks;
+    key.dyn = dyn;
+    key.A = A;
+    if (!kgraph_exec_ || kgraph_key_.size() != sizeof key || std::memcmp(kgraph_key_.data(), &key, sizeof key) != 0) {
+        if (kgraph_exec_) cudaGraphExecDestroy((cudaGraphExec_t)kgraph_exec_);
+        kgraph_exec_ = nullptr;
+        cudaGraph_t gr = nullptr;
+        cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        cudaMemsetAsync(A.counter, 0, 4, s);
+        if (stat) {
+            if (dense) k_batch<4, true, 4><<<blocks, 4 * 32, dyn, s>>>(A);
+            else k_batch<4, true, 3><<<blocks, 4 * 32, dyn, s>>>(A);
+        } else {
+            if (dense) k_batch<4, false, 4><<<blocks, 4 * 32, dyn, s>>>(A);
+            else k_batch<4, false, 3><<<blocks, 4 * 32, dyn, s>>>(A);
+        }
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(s, &gr);
+        cuda_check(le, "k_batch launch");
+        cuda_check(ce, "end capture");
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        cuda_check(ie, "graph instantiate");
+        kgraph_exec_ = ex;
+        kgraph_key_.assign((const char*)&key, (const char*)&key + sizeof key);
     }
-    cuda_check(cudaGetLastError(), "k_batch launch");
+    cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "event");
+    cuda_check(cudaGraphLaunch((cudaGraphExec_t)kgraph_exec_, s), "k_batch graph launch");
     cuda_check(cudaEventRecord((cudaEvent_t)ev1_, s), "event");
     cuda_check(cudaEventSynchronize((cudaEvent_t)ev1_), "k_batch");
     float ms = 0.f;

@@ -103,9 +103,13 @@ class BatchEngine {
     };
     Caps default_caps(int scale) const;
     int ring_blocks() const;
-    // one persistent launch over `count` windows (ids) with slots of the given capacities
-    void launch(const int32_t* windows, int32_t count, const Caps& caps);
+    // one persistent launch over `count` windows (ids) with slots of the given
+    // capacities, grown by up to `headroom` when memory allows every resident warp one
+    void launch(const int32_t* windows, int32_t count, const Caps& caps, double headroom = 1.0);
+    static constexpr double PLAN_HEADROOM = 1.5;
     Proposer* proposer_ = nullptr;
+    void* kgraph_exec_ = nullptr;      // the launch as a CUDA graph, and the launch it was recorded for
+    std::vector<char> kgraph_key_;
     void* evr0_ = nullptr;
     void* evr1_ = nullptr;
     void* evp_ = nullptr;

@@ -525,6 +525,7 @@ Proposer::Proposer(int device) : device_(device) {
 
 Proposer::~Proposer() {
     cudaSetDevice(device_);
+    if (graph_exec_) cudaGraphExecDestroy((cudaGraphExec_t)graph_exec_);
     for (void* p : {(void*)d_w_, (void*)d_wb_, (void*)d_g_, (void*)d_m_, (void*)d_v_, (void*)d_extra_, d_act_, d_tab_,
                     d_plan_, (void*)d_feat_, (void*)d_pred_})
         if (p) cudaFree(p);
@@ -677,10 +678,16 @@ float Proposer::train(const float* X, const float* Y, int64_t n, int epochs, int
     return last;
 }
 
+constexpr int64_t PREDICT_CHUNK = 4096;
+
 void Proposer::predict_device(const float* dX, int64_t n, float* dY, void* stream) {
+    ensure(std::min<int64_t>(std::max<int64_t>(n, 1), PREDICT_CHUNK));
+    predict_launch(dX, n, dY, stream);
+}
+
+// the inference launches only (buffers already sized by ensure)
+void Proposer::predict_launch(const float* dX, int64_t n, float* dY, void* stream) {
     cudaStream_t s = (cudaStream_t)stream;
-    constexpr int64_t CHUNK = 4096;
-    ensure(std::min<int64_t>(std::max<int64_t>(n, 1), CHUNK));
     Act a;
     act_layout(cap_, &a, (char*)d_act_);
     for (int64_t b0 = 0; b0 < n; b0 += cap_) {
@@ -705,10 +712,23 @@ void Proposer::predict_host(const float* X, int64_t n, float* Y) {
 }
 
 void Proposer::features(const DeviceWindows& dw, int k, int w, float* dX, void* stream) {
+    if (dw.n_windows <= 0) return;
+    int bits = 0, grid = 0;
+    features_prep(dw, k, w, bits, grid);
+    features_launch(dw, k, w, bits, grid, dX, stream);
+}
+
+void Proposer::features_launch(const DeviceWindows& dw, int k, int w, int bits, int grid, float* dX, void* stream) {
+    k_features<<<grid, FT_THREADS, 0, (cudaStream_t)stream>>>(dw.seq, dw.read_off, dw.read_len, dw.win_off,
+                                                               dw.n_windows, k, w, (unsigned long long*)d_tab_, bits,
+                                                               dX);
+    cuda_check(cudaGetLastError(), "k_features");
+}
+
+// hash-table size and grid of the feature kernel; allocates its scratch
+void Proposer::features_prep(const DeviceWindows& dw, int k, int w, int& bits_out, int& grid_out) {
     if (k < 1 || k > FT_MAXK || w < 1 || w > FT_MAXW) throw std::invalid_argument("proposer: k or w out of range");
     cuda_check(cudaSetDevice(device_), "cudaSetDevice");
-    cudaStream_t s = (cudaStream_t)stream;
-    if (dw.n_windows <= 0) return;
     // table: at least twice the window's possible minimizers, a power of two
     const double est = (double)dw.max_win_bases * 2.0 / (w + 1) * 1.5 + 1024.0;
     int bits = 10;
@@ -729,9 +749,8 @@ void Proposer::features(const DeviceWindows& dw, int k, int w, float* dX, void* 
         cuda_check(cudaMalloc(&d_tab_, need), "cudaMalloc(proposer tables)");
         tab_bytes_ = need;
     }
-    k_features<<<grid, FT_THREADS, 0, s>>>(dw.seq, dw.read_off, dw.read_len, dw.win_off, dw.n_windows, k, w,
-                                           (unsigned long long*)d_tab_, bits, dX);
-    cuda_check(cudaGetLastError(), "k_features");
+    bits_out = bits;
+    grid_out = grid;
 }
 
 void Proposer::plan(const DeviceWindows& dw, int k, int w, std::vector<int32_t>& nodes, std::vector<int64_t>& tb,
@@ -765,15 +784,42 @@ void Proposer::plan(const DeviceWindows& dw, int k, int w, std::vector<int32_t>&
     spill.assign(nw, 0);
     cost.assign(nw, 0.f);
     if (nw == 0) return;
-    features(dw, k, w, d_feat_, s);
-    predict_device(d_feat_, dw.n_reads, d_pred_, s);
+    int bits = 0, grid = 0;
+    features_prep(dw, k, w, bits, grid);
+    ensure(std::min<int64_t>(std::max<int64_t>(dw.n_reads, 1), PREDICT_CHUNK));
     char* p = (char*)d_plan_;
     int32_t* dn = (int32_t*)p;
     int64_t* dt = (int64_t*)(p + up256(4 * (size_t)nw));
     int64_t* ds = (int64_t*)(p + up256(4 * (size_t)nw) + up256(8 * (size_t)nw));
     float* dc = (float*)(p + up256(4 * (size_t)nw) + 2 * up256(8 * (size_t)nw));
-    k_plan<<<grid_of(nw), 256, 0, s>>>(d_pred_, dw.read_len, dw.win_off, nw, d_extra_, dn, dt, ds, dc);
-    cuda_check(cudaGetLastError(), "k_plan");
+    // features, inference and plan: ~10 launches per 4,096 reads, recorded once as a
+    // CUDA graph per batch shape and replayed with one launch
+    const GraphKey key{dw.seq, dw.read_off, dw.read_len, dw.win_off, dw.n_reads, nw, k, w, bits, grid,
+                       d_feat_, d_pred_, d_plan_, d_tab_, d_act_, cap_, s};
+    if (!graph_exec_ || std::memcmp(&key, &graph_key_, sizeof key) != 0) {
+        if (graph_exec_) cudaGraphExecDestroy((cudaGraphExec_t)graph_exec_);
+        graph_exec_ = nullptr;
+        cudaGraph_t gr = nullptr;
+        cuda_check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+        try {
+            features_launch(dw, k, w, bits, grid, d_feat_, s);
+            predict_launch(d_feat_, dw.n_reads, d_pred_, s);
+            k_plan<<<grid_of(nw), 256, 0, s>>>(d_pred_, dw.read_len, dw.win_off, nw, d_extra_, dn, dt, ds, dc);
+            cuda_check(cudaGetLastError(), "k_plan");
+        } catch (...) {
+            cudaStreamEndCapture(s, &gr);
+            if (gr) cudaGraphDestroy(gr);
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(s, &gr), "end capture");
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        cuda_check(e, "graph instantiate");
+        graph_exec_ = ex;
+        std::memcpy(&graph_key_, &key, sizeof key);
+    }
+    cuda_check(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, s), "graph launch");
     cuda_check(cudaMemcpyAsync(nodes.data(), dn, 4 * (size_t)nw, cudaMemcpyDeviceToHost, s), "D2H plan");
     cuda_check(cudaMemcpyAsync(tb.data(), dt, 8 * (size_t)nw, cudaMemcpyDeviceToHost, s), "D2H plan");
     cuda_check(cudaMemcpyAsync(spill.data(), ds, 8 * (size_t)nw, cudaMemcpyDeviceToHost, s), "D2H plan");

@@ -82,6 +82,20 @@ class Proposer {
     float extra(int i) const { return host_w_[PROP_NPARAM + i]; }
 
   private:
+    // the plan's launches are replayed from a CUDA graph while these stay the same
+    struct GraphKey {
+        const void *seq, *read_off, *read_len, *win_off;
+        int64_t n_reads;
+        int32_t n_windows, k, w, bits, grid;
+        const void *feat, *pred, *plan, *tab, *act;
+        int64_t cap;
+        const void* stream;
+    };
+    void features_prep(const DeviceWindows& dw, int k, int w, int& bits, int& grid);
+    void features_launch(const DeviceWindows& dw, int k, int w, int bits, int grid, float* dX, void* stream);
+    void predict_launch(const float* dX, int64_t n, float* dY, void* stream);
+    void* graph_exec_ = nullptr;
+    GraphKey graph_key_{};
     void ensure(int64_t batch_reads);
     void forward(const float* dX, int64_t n, void* stream);
     void upload_bf16(void* stream);

@@ -134,3 +134,19 @@ def test_batch_capacity_retry():
     solo = poa_b200.run(big.window_reads(0))
     assert b">consensus sequence\n" + cons[-1] + b"\n" == solo
     print("retried", stats["retried"], "launches", stats["launches"])
+
+
+def test_autotune_small(tmp_path):
+    """The launch-shape autotuner runs every candidate on a small sample, picks one,
+    and a tuned context gives the same consensus as the default shape."""
+    from poa_b200 import autotune
+    t = autotune.tune("polishing", windows=300, log=lambda *a: None)
+    assert (t["blocks_per_sm"], t["smem_per_warp"]) in autotune.CANDIDATES
+    assert len(t["measured"]) >= 1
+    ws = synth.polishing_windows(seed=33, n_windows=50)
+    with poa_b200.Context() as ctx:
+        cons0, st0 = ctx.batch_consensus(ws)
+        ctx.batch_config(blocks_per_sm=t["blocks_per_sm"], smem_per_warp=t["smem_per_warp"])
+        cons1, st1 = ctx.batch_consensus(ws)
+        cons2, st2 = ctx.batch_consensus(ws)  # replayed launch graph
+    assert st0 == [0] * 50 and cons1 == cons0 and st1 == st0 and cons2 == cons0

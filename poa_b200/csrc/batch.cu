@@ -831,7 +831,7 @@ __device__ __forceinline__ const int32_t* blk_src(const int32_t* ring, const int
 // er_base[cur.e0 + k] in the backtrack's priority order. Predecessor blocks
 // come from blk_src (the shared-memory ring or the slot's row store). With
 // ARGMAX, each lane also keeps the first maximum of M over its cells.
-template <bool ARGMAX>
+template <bool ARGMAX, bool TRACK>
 __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, const int4* __restrict__ er_base,
                                          const int32_t* ring, int RB, const uint8_t* __restrict__ qsm, int i,
                                          int lane, int32_t& bestM, int& bestJ) {
@@ -848,11 +848,19 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
         const int B = Bs + b;
         const int j0 = b * BLK;
         int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
-        int32_t cMb[BLK], cDb[BLK], cmprev = NEG_INF;
-        bool c_blk = false, c_prev = false;
+        // X, Y: with one predecessor, its M and D at this block (for the records);
+        // with several and TRACK, the record choices kept while the predecessors
+        // are read: X = m1 | m4 << 16 (first predecessors, in priority order,
+        // reaching the diagonal maximum), Y = dopen | dext << 16 (the vertical
+        // maximum); 511 = none
+        uint32_t X[BLK], Y[BLK];
+        int32_t cmprev = NEG_INF;
+        bool c_blk = false, c_prev = false, slow = !TRACK, slow0 = false;
+        uint32_t hm = 0;  // bit l: Mpre[l] >= Dv[l], then (after the scan) M[l] == Mpre[l]
         uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
+        const uint32_t xinit = (TRACK && d >= 2) ? 0x01ff01ffu : (uint32_t)NEG_INF;
 #pragma unroll
-        for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; cMb[l] = cDb[l] = NEG_INF; }
+        for (int l = 0; l < BLK; l++) { Mpre[l] = NEG_INF; Dv[l] = NEG_INF; X[l] = Y[l] = xinit; }
         if (act) {
             const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
             qlo = qw.x;
@@ -870,14 +878,59 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
                 if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
                 if (mk.blk_in) {
                     load_block16(src + (B - pBs) * 16, Mb, Db);
-                    uint8_t qc8[BLK];
+                    if (TRACK && d >= 2) {
+                        // the maxima of pass1_pred, keeping the first predecessor (in
+                        // priority order) that reaches each final maximum
+                        const int4 erk = er_base[cur.e0 + k];
+                        const uint32_t pos = (uint32_t)erk.z >> 16;
+                        const uint32_t m1v = (erk.w & 256) ? pos : 510u;
 #pragma unroll
-                    for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qlo >> (8 * l)); qc8[4 + l] = (uint8_t)(qhi >> (8 * l)); }
-                    pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
-                    if (d == 1) {
+                        for (int l = 0; l < BLK; l++) {
+                            const int32_t co = add32(Mb[l], sc.o1), ce = add32(Db[l], sc.e1);
+                            const int32_t nd = mx(Dv[l], mx(co, ce));
+                            if (nd > Dv[l]) {
+                                Y[l] = (co == nd ? pos : 511u) | ((ce == nd ? pos : 511u) << 16);
+                            } else {
+                                if ((Y[l] & 0xffffu) == 511u && co == nd) Y[l] = (Y[l] & 0xffff0000u) | pos;
+                                if ((Y[l] >> 16) == 511u && ce == nd) Y[l] = (Y[l] & 0xffffu) | (pos << 16);
+                            }
+                            Dv[l] = nd;
+                        }
+                        if (mk.diag) {
 #pragma unroll
-                        for (int l = 0; l < BLK; l++) { cMb[l] = Mb[l]; cDb[l] = Db[l]; }
+                            for (int l = 0; l < BLK; l++) {
+                                const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
+                                const bool bm = pbase == qc;
+                                const int32_t src0 = l == 0 ? (b == 0 ? NEG_INF : mprev) : Mb[l > 0 ? l - 1 : 0];
+                                const int32_t cand = add32(src0, bm ? sc.match : sc.mismatch);
+                                const bool tracked = l > 0 || b != 0;  // the backtrack tests this same value
+                                if (cand > Mpre[l]) {
+                                    X[l] = tracked ? ((bm ? m1v : 511u) | (pos << 16)) : 0x01ff01ffu;
+                                } else if (tracked && cand == Mpre[l]) {
+                                    if ((X[l] >> 16) == 511u) X[l] = (X[l] & 0xffffu) | (pos << 16);
+                                    if (bm && (X[l] & 0xffffu) == 511u) X[l] = (X[l] & 0xffff0000u) | m1v;
+                                }
+                                Mpre[l] = mx(Mpre[l], cand);
+                            }
+                        }
+                    } else {
+                        uint8_t qc8[BLK];
+#pragma unroll
+                        for (int l = 0; l < 4; l++) { qc8[l] = (uint8_t)(qlo >> (8 * l)); qc8[4 + l] = (uint8_t)(qhi >> (8 * l)); }
+                        pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+                        if (d == 1) {
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) { X[l] = (uint32_t)Mb[l]; Y[l] = (uint32_t)Db[l]; }
+                        }
                     }
+                }
+                // where the backtrack's predecessor test and the fill's block-granular
+                // diagonal differ (a predecessor's band starting in this block, or ending
+                // just before it, or the row's first block), the choices are redone with
+                // the backtrack's own test: the whole block in the first case, cell 0 else
+                if (TRACK && d >= 2) {
+                    slow |= mk.blk_in && !mk.diag;
+                    slow0 |= mk.prev_in && !(mk.blk_in && mk.diag && b != 0);
                 }
                 if (d == 1) { cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in; }
             }
@@ -887,6 +940,7 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
 #pragma unroll
         for (int l = 0; l < BLK; l++) {
             H0[l] = mx(Mpre[l], Dv[l]);
+            if (TRACK && Mpre[l] >= Dv[l]) hm |= 1u << l;
             agg = mx(agg, add32(H0[l], -(j0 + l) * sc.e1));
         }
         if (!act) agg = INT_MIN;
@@ -904,6 +958,7 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
             for (int l = 0; l < BLK; l++) {
                 I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
                 M[l] = mx(H0[l], I[l]);
+                if (TRACK && H0[l] < I[l]) hm &= ~(1u << l);
                 run = mx(run, add32(H0[l], -(j0 + l) * sc.e1));
             }
         }
@@ -927,13 +982,13 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
                     if (d == 1) {
                         const int qc = (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255);
                         const bool inr = l == 0 ? c_prev : c_blk;
-                        const int32_t mv = l == 0 ? cmprev : cMb[l > 0 ? l - 1 : 0];
+                        const int32_t mv = l == 0 ? cmprev : (int32_t)X[l > 0 ? l - 1 : 0];
                         const bool bm = cur.pbase == qc;
                         const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
                         if (eqM) r |= R_M4;
                         if (eqM && bm && cur.w1ok) r |= R_M1;
-                        if (c_blk && Dv[l] == add32(cMb[l], sc.o1)) r |= R_DOPEN;
-                        else if (c_blk && Dv[l] == add32(cDb[l], sc.e1)) r |= R_DEXT;
+                        if (c_blk && Dv[l] == add32((int32_t)X[l], sc.o1)) r |= R_DOPEN;
+                        else if (c_blk && Dv[l] == add32((int32_t)Y[l], sc.e1)) r |= R_DEXT;
                     }
                     if (l < 4) lo |= r << (8 * l);
                     else hi |= r << (8 * (l - 4));
@@ -942,10 +997,35 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
             } else {
                 // choices per cell: m1 | m4 << 16, dopen | dext << 16 (511 = none,
                 // 510 = the best matching predecessor failed the weight threshold)
-                uint32_t cm[BLK], cd[BLK];
+                uint32_t* cm = X;
+                uint32_t* cd = Y;
+                if (!slow) {
+                    // tracked choices stand where M is the diagonal maximum itself
 #pragma unroll
-                for (int l = 0; l < BLK; l++) { cm[l] = 0x01ff01ffu; cd[l] = 0x01ff01ffu; }
-                for (int k = 0; k < d; k++) {
+                    for (int l = 0; l < BLK; l++)
+                        if (!((hm >> l) & 1u)) cm[l] = 0x01ff01ffu;
+                    if (slow0) {
+                        // cell 0 by the backtrack's own test, over every predecessor
+                        uint32_t c0 = 0x01ff01ffu;
+                        const int qc = (int)(qlo & 255u);
+                        for (int k = 0; k < d; k++) {
+                            const int4 er = er_base[cur.e0 + k];
+                            const int pBs = er.x & 0xffff, pBe = er.x >> 16;
+                            if (!(B - 1 >= pBs && B - 1 <= pBe - 2)) continue;  // prev_in
+                            const int32_t mv = blk_src(ring, a.rs, RB, er.y)[(B - 1 - pBs) * 16 + 7];
+                            const uint32_t pos = (uint32_t)er.z >> 16;
+                            const bool bm = (er.w & 255) == qc;
+                            if (M[0] != add32(mv, bm ? sc.match : sc.mismatch)) continue;
+                            if ((c0 >> 16) == 511u) c0 = (c0 & 0xffffu) | (pos << 16);
+                            if (bm && (c0 & 0xffffu) == 511u) c0 = (c0 & 0xffff0000u) | ((er.w & 256) ? pos : 510u);
+                        }
+                        cm[0] = c0;
+                    }
+                }
+#pragma unroll
+                for (int l = 0; l < BLK; l++)
+                    if (slow) { cm[l] = 0x01ff01ffu; cd[l] = 0x01ff01ffu; }
+                for (int k = 0; k < (slow ? d : 0); k++) {
                     const int4 er = er_base[cur.e0 + k];
                     const int pBs = er.x & 0xffff, pBe = er.x >> 16;
                     const int32_t* src = blk_src(ring, a.rs, RB, er.y);
@@ -1036,7 +1116,7 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
             ecells += rc * cur.d;
             int32_t bm = 0;
             int bj = 0;
-            fill_row<false>(a, cur, er_base, ring, RB, qsm, i, lane, bm, bj);
+            fill_row<false, false>(a, cur, er_base, ring, RB, qsm, i, lane, bm, bj);
             __syncwarp();
         }
     }
@@ -1303,8 +1383,8 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
         }
         int32_t bestM = INT_MIN;
         int bestJ = 0;
-        if (adaptive) fill_row<true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
-        else fill_row<false>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
+        if (adaptive) fill_row<true, true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
+        else fill_row<false, true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
         cells += (int64_t)bn * BLK;
         ecells += (int64_t)bn * BLK * d;
         if (adaptive && i >= 1) {

@@ -150,3 +150,20 @@ def test_autotune_small(tmp_path):
         cons1, st1 = ctx.batch_consensus(ws)
         cons2, st2 = ctx.batch_consensus(ws)  # replayed launch graph
     assert st0 == [0] * 50 and cons1 == cons0 and st1 == st0 and cons2 == cons0
+
+
+@pytest.mark.parametrize("opts", [[], ["-B"]])
+def test_batch_empty_windows(opts):
+    """Windows without reads, or with one empty read, give the empty consensus,
+    as minipoa does on such input; their neighbours are unaffected."""
+    _, w0 = fasta.read(os.path.join(GOLD, "window_00.fa"))
+    reads = list(w0) + [b""] + [b"ACGT"]
+    offs = [0, len(w0), len(w0), len(w0) + 1, len(w0) + 2]
+    ws = synth.pack_windows_from_reads(reads, offs)
+    with poa_b200.Context(poa_b200.Params.from_cli(opts)) as ctx:
+        cons, st = ctx.batch_consensus(ws)
+        text0, _ = ctx.run(list(w0), None)
+    assert st == [0, 0, 0, 0]
+    assert cons[0] == text0.split(b"\n")[1]
+    assert cons[1] == b"" and cons[2] == b""
+    assert cons[3] == b"ACGT"

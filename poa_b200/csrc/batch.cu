@@ -1215,80 +1215,6 @@ __device__ void adaptive_update_pf(const DpArgs& a, int i, int Bs, int max_j, in
     __syncwarp();
 }
 
-// adaptive_update (dp_rowops.h, src/align.cpp:1516-1568) with the warp: the
-// predecessors' slope test and the successors' band updates run one lane per
-// edge (successors are distinct rows, so their updates do not collide); lane 0
-// settles row i's own state in between. Same results as the serial version.
-__device__ void adaptive_update_warp(const DpArgs& a, int i, int Bs, int max_j, int lane) {
-    const int n = a.v.n;
-    int32_t* Mp = a.state + AB_MP * n;
-    int32_t* Sl = a.state + AB_SL * n;
-    int32_t* Pl = a.state + AB_PL * n;
-    int32_t* Pr = a.state + AB_PR * n;
-    int32_t* Ol = a.state + AB_OL * n;
-    int32_t* Or = a.state + AB_OR * n;
-    int32_t* Ow = a.state + AB_OW * n;
-    const int max_acj = Bs * BLK + max_j;
-    const bool base_match = (int)a.v.base[i] == (int)a.qs[max_acj + 1];  // cur.base == seq[max_acj]
-    int sl_best = INT_MIN, max_slp = 0;
-    bool is_match = false;
-    if (base_match) {
-        const int e0 = a.v.in_ptr[i], e1 = a.v.in_ptr[i + 1];
-        for (int e = e0 + lane; e < e1; e += 32) {
-            const int p = a.v.in_row[e];
-            const int slp = Sl[p];
-            max_slp = max(max_slp, slp);
-            if (Mp[p] + 1 == max_acj) {
-                is_match = true;
-                sl_best = max(sl_best, slp + 1);
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
-            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
-        }
-        is_match = __any_sync(0xffffffffu, is_match);
-    }
-    int sl_i = 0, ow_i = 0, ol_i = 0, or_i = 0;
-    if (lane == 0) {
-        Mp[i] = max_acj;
-        sl_i = Sl[i];
-        ow_i = Ow[i];
-        ol_i = Ol[i];
-        or_i = Or[i];
-        if (is_match) sl_i = mx(sl_i, sl_best);
-        if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
-        if (sl_i >= 30) {
-            ol_i = or_i = max_acj - a.v.hq_loc[i];
-            ow_i = 0;
-        }
-        Sl[i] = sl_i;
-        Ow[i] = ow_i;
-        Ol[i] = ol_i;
-        Or[i] = or_i;
-    }
-    sl_i = __shfl_sync(0xffffffffu, sl_i, 0);
-    ow_i = __shfl_sync(0xffffffffu, ow_i, 0);
-    ol_i = __shfl_sync(0xffffffffu, ol_i, 0);
-    or_i = __shfl_sync(0xffffffffu, or_i, 0);
-    const int o0 = a.v.out_ptr[i], o1 = a.v.out_ptr[i + 1];
-    for (int e = o0 + lane; e < o1; e += 32) {
-        const int s = a.v.out_row[e];
-        if (sl_i >= 30) {
-            Ol[s] = ol_i;
-            Or[s] = or_i;
-        } else {
-            Ol[s] = mn(Ol[s], ol_i);
-            Or[s] = mx(Or[s], or_i);
-        }
-        Pl[s] = mn(Pl[s], max_acj);
-        Pr[s] = mx(Pr[s], max_acj + 1);
-        Ow[s] = ow_i ? mx(Ow[s], ow_i) : ow_i;
-    }
-    __syncwarp();
-}
-
 __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const int32_t* __restrict__ vmaxs,
                                  const uint8_t* __restrict__ qsm, int4* sed, int32_t* upd, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
@@ -1610,8 +1536,7 @@ __device__ int build_view(DevGraph& g, char* s, const SlotLayout& L, WinView& v,
 }
 
 template <bool STATIC>
-__device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared* sr, unsigned char* wsm, int w,
-                               int lane) {
+__device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, unsigned char* wsm, int w, int lane) {
     const SlotLayout& L = A.L;
     DevGraph g = slot_graph(s, L);
     const int r0 = A.win_off[w], r1 = A.win_off[w + 1];
@@ -1635,7 +1560,6 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
         g.hdr[1] = 0;
     }
     __syncwarp();
-    WarpGroup grp{sr};
     for (int r = r0; r < r1 && status == ST_OK; r++) {
         const uint8_t* rd = A.seq + A.read_off[r];
         const int len = A.read_len[r];
@@ -1820,7 +1744,6 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, RowShared
 template <int WARPS, bool STATIC, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_batch(BatchArgs A) {
     __shared__ DpArgs s_args[WARPS];
-    __shared__ RowShared s_sr[WARPS];
     extern __shared__ __align__(16) unsigned char dsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * WARPS + warp;
@@ -1831,7 +1754,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_batch(BatchArgs A) {
         if (lane == 0) idx = atomicAdd(A.counter, 1);
         idx = __shfl_sync(0xffffffffu, idx, 0);
         if (idx >= A.n_windows) break;
-        process_window<STATIC>(A, s, s_args[warp], &s_sr[warp], wsm, A.order[idx], lane);
+        process_window<STATIC>(A, s, s_args[warp], wsm, A.order[idx], lane);
     }
 }
 

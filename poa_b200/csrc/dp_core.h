@@ -153,6 +153,14 @@ PB_UNROLL
 // A[k] = H0[k] - k*e1 for the prefix-max form of the I recurrence.
 PB_HD int32_t scan_key(int32_t h0, int j, int32_t e1) { return add32(h0, -(int32_t)((int64_t)j * e1)); }
 
+// I at column j >= 1 from the prefix max `run` of the scan keys of the cells
+// left of j.
+PB_HD int32_t i_at(const Scoring& s, int j, int32_t run) {
+    int32_t ext = add32(NEG_INF, (int32_t)((int64_t)j * s.e1));
+    int32_t opn = add32(add32(s.o1, (int32_t)((int64_t)(j - 1) * s.e1)), run);
+    return mx(ext, opn);
+}
+
 // Finalise M and I of one block given H0 and the exclusive prefix max P of the
 // scan keys of all cells left of the block (ignored when the block holds j=0).
 PB_HD void finalize_block(const Scoring& s, int j0, int32_t P, const int32_t* H0, int32_t* M, int32_t* I) {
@@ -161,20 +169,22 @@ PB_HD void finalize_block(const Scoring& s, int j0, int32_t P, const int32_t* H0
 PB_UNROLL
     for (int l = 0; l < BLK; l++) {
         int j = j0 + l;
-        int32_t Ij;
-        if (j == 0) {
-            Ij = NEG_INF;
-        } else {
-            int32_t ext = add32(NEG_INF, (int32_t)((int64_t)j * s.e1));
-            int32_t opn = add32(add32(s.o1, (int32_t)((int64_t)(j - 1) * s.e1)), run);
-            Ij = mx(ext, opn);
-        }
+        int32_t Ij = j == 0 ? NEG_INF : i_at(s, j, run);
         I[l] = Ij;
         M[l] = mx(H0[l], Ij);
         int32_t key = scan_key(H0[l], j, s.e1);
         run = have ? mx(run, key) : key;
         have = true;
     }
+}
+
+// M and I of the last cell of a block (j0 + 7) without the block's other
+// cells: P as for finalize_block, k06 = max of the scan keys of its cells
+// 0..6, h07 = its H0[7]. Equal to finalize_block's M[7], I[7].
+PB_HD void finalize_last(const Scoring& s, int j0, int32_t P, int32_t k06, int32_t h07, int32_t& M7, int32_t& I7) {
+    const int32_t run = j0 > 0 ? mx(P, k06) : k06;
+    I7 = i_at(s, j0 + BLK - 1, run);
+    M7 = mx(h07, I7);
 }
 
 // Per-cell best-so-far keys for multi-predecessor records: (weight << 10) |

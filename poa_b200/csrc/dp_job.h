@@ -44,7 +44,9 @@ struct DpArgs {
     // int32 are a ring of recent rows (row i in slot i % ring_rows). A row goes
     // to the spill area after the ring (bump-allocated) instead when one of its
     // in-window successors is ring_rows or more rows ahead, or when it is wider
-    // than ring_blocks. ring_rows == 0 stores every row linearly.
+    // than ring_blocks. ring_rows == 0 stores every row linearly. The static-band
+    // plain kernel (plain_static.cuh) keeps its ring in shared memory instead
+    // and stores only the other rows here, linearly.
     int32_t ring_rows, ring_blocks;
     uint8_t* tb;         // traceback records
     int64_t tb_cap;      // bytes

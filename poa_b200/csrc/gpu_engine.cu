@@ -8,6 +8,7 @@
 #include <stdexcept>
 
 #include "plain.cuh"
+#include "plain_static.cuh"
 
 namespace pb {
 
@@ -52,11 +53,35 @@ void launch_plain(int njobs, const DpArgs* d_jobs, cudaStream_t s) {
     k_plain<NT><<<njobs, NT, 0, s>>>(d_jobs);
 }
 
-void launch_by_width(int est_blocks, int njobs, const DpArgs* d_jobs, cudaStream_t s) {
-    if (est_blocks <= 32) launch_plain<32>(njobs, d_jobs, s);
-    else if (est_blocks <= 64) launch_plain<64>(njobs, d_jobs, s);
-    else if (est_blocks <= 128) launch_plain<128>(njobs, d_jobs, s);
-    else if (est_blocks <= 256) launch_plain<256>(njobs, d_jobs, s);
+// Shared memory for the static kernel's row ring (below the 227 KB a block
+// may use, leaving part of the unified L1 for the read-only window arrays).
+// The adaptive kernel keeps its rows in global memory: a shared-memory ring
+// of a few full-width rows measured slower there (less L1 for the rest).
+constexpr int kRingBytes = 160 * 1024;
+constexpr int kRingMaxRows = 32;
+
+template <int NT>
+void launch_static(int njobs, const DpArgs* d_jobs, size_t dyn, cudaStream_t s) {
+    if (dyn > 48 * 1024)
+        cuda_check(cudaFuncSetAttribute(k_plain_static<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn),
+                   "smem attr (k_plain_static)");
+    k_plain_static<NT><<<njobs, NT, dyn, s>>>(d_jobs);
+}
+
+void launch_static_by_width(int max_bn, int njobs, const DpArgs* d_jobs, size_t dyn, cudaStream_t s) {
+    if (max_bn <= 64) launch_static<64>(njobs, d_jobs, dyn, s);
+    else if (max_bn <= 128) launch_static<128>(njobs, d_jobs, dyn, s);
+    else if (max_bn <= 192) launch_static<192>(njobs, d_jobs, dyn, s);
+    else if (max_bn <= 256) launch_static<256>(njobs, d_jobs, dyn, s);
+    else if (max_bn <= 384) launch_static<384>(njobs, d_jobs, dyn, s);
+    else launch_static<512>(njobs, d_jobs, dyn, s);
+}
+
+void launch_by_width(int max_bn, int njobs, const DpArgs* d_jobs, cudaStream_t s) {
+    if (max_bn <= 32) launch_plain<32>(njobs, d_jobs, s);
+    else if (max_bn <= 64) launch_plain<64>(njobs, d_jobs, s);
+    else if (max_bn <= 128) launch_plain<128>(njobs, d_jobs, s);
+    else if (max_bn <= 256) launch_plain<256>(njobs, d_jobs, s);
     else launch_plain<512>(njobs, d_jobs, s);
 }
 
@@ -122,7 +147,8 @@ void GpuEngine::align_many(const std::vector<const HostWindow*>& wins, const std
     };
     std::vector<Lay> L(J);
     size_t up = up16(sizeof(DpArgs) * J);
-    int est_blocks = 1;
+    int max_bn_all = 1;
+    bool any_adaptive = false;
     for (int t = 0; t < J; t++) {
         const HostWindow& w = *wins[t];
         const int n = w.n, E = (int)w.in_row.size(), E2 = (int)w.out_row.size();
@@ -144,8 +170,11 @@ void GpuEngine::align_many(const std::vector<const HostWindow*>& wins, const std
         const bool adaptive = p.f > 0 && abs[t];
         int max_bn;
         job_capacity(w, qlens[t], adaptive, p.f, l.w, l.rs_cap, l.tb_cap, max_bn);
-        int est = adaptive ? std::min(max_bn, 2 * l.w / BLK + 3) : max_bn;
-        est_blocks = std::max(est_blocks, est);
+        // the CTA covers the widest row in one chunk (up to 512 threads): an
+        // adaptive row can widen to the full query (max_bn = m/8 + 2), and
+        // idle threads cost less than extra chunks, each a serial scan step
+        max_bn_all = std::max(max_bn_all, max_bn);
+        any_adaptive = any_adaptive || adaptive;
         l.moves_cap = n + m + 8;
     }
     size_t res_begin = up;
@@ -164,6 +193,15 @@ void GpuEngine::align_many(const std::vector<const HostWindow*>& wins, const std
     }
     reserve_device(pos);
     reserve_host(res_end);
+
+    // static bands only: k_plain_static with a shared-memory ring of recent rows
+    int ring_rows = 0;
+    if (!any_adaptive) {
+        ring_rows = std::min(kRingMaxRows, kRingBytes / (max_bn_all * 64));
+        if (ring_rows < 2) ring_rows = 0;
+    }
+    const int ring_blocks = max_bn_all;
+    const size_t ring_bytes = (size_t)ring_rows * ring_blocks * 64;
 
     char* h = hbuf_;
     char* d = dbuf_;
@@ -212,6 +250,8 @@ void GpuEngine::align_many(const std::vector<const HostWindow*>& wins, const std
         a.rs_cap = l.rs_cap;
         a.tb = reinterpret_cast<uint8_t*>(d + l.tb);
         a.tb_cap = l.tb_cap;
+        a.ring_rows = ring_rows;
+        a.ring_blocks = ring_rows > 0 ? ring_blocks : 0;
         a.out = reinterpret_cast<int32_t*>(d + l.res);
         a.moves = reinterpret_cast<int32_t*>(d + l.res + 16);
         a.moves_cap = l.moves_cap;
@@ -219,7 +259,8 @@ void GpuEngine::align_many(const std::vector<const HostWindow*>& wins, const std
     }
     cuda_check(cudaMemcpyAsync(d, h, res_begin, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(H2D)");
     if (timing) cuda_check(cudaEventRecord((cudaEvent_t)ev0_, s), "cudaEventRecord");
-    launch_by_width(est_blocks, J, reinterpret_cast<const DpArgs*>(d), s);
+    if (any_adaptive) launch_by_width(max_bn_all, J, reinterpret_cast<const DpArgs*>(d), s);
+    else launch_static_by_width(max_bn_all, J, reinterpret_cast<const DpArgs*>(d), ring_bytes, s);
     cuda_check(cudaGetLastError(), "k_plain launch");
     if (timing) cuda_check(cudaEventRecord((cudaEvent_t)ev1_, s), "cudaEventRecord");
     cuda_check(cudaMemcpyAsync(h + res_begin, d + res_begin, res_end - res_begin, cudaMemcpyDeviceToHost, s),

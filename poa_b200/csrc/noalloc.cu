@@ -65,10 +65,10 @@ __global__ void __launch_bounds__(NT, 1) k_plain_noalloc(DpArgs a, const uint8_t
         return;
     }
     constexpr int NW = NT / 32;
-    __shared__ int32_t s_scan[NW], s_scan2[NW], s_lastM[NW], s_lastI[NW];
+    __shared__ int4 s_sum[2 * NW];
     __shared__ unsigned long long s_key[NW];
-    __shared__ RowShared sr;
-    CtaGroup<NT> g{s_scan, s_scan2, s_lastM, s_lastI, s_key, &sr};
+    __shared__ RowShared sr[2];
+    CtaGroup<NT> g{s_sum, s_key, sr};
     dp_fill(g, a);
     __syncthreads();
     if (threadIdx.x == 0 && a.out[0] == ST_OK) {

@@ -8,12 +8,16 @@
 //      loads p's M/D block (64 B, coalesced across the CTA) plus one M cell to
 //      its left, and folds the diagonal and vertical terms (pass1_pred).
 //   2. the horizontal gap recurrence is a CTA-wide exclusive prefix max of
-//      H0[k] - k*e1 (warp shuffles + one shared-memory level).
+//      H0[k] - k*e1 (warp shuffles + one barrier, CtaGroup::scan).
 //   3. final M and I, the backtrack records of the block (own-row tests plus
-//      one comparison sweep over the predecessors), and the row's M/D blocks
-//      are written back to global memory, all 16-byte vector stores.
-//   4. with the adaptive band, a CTA argmax of M, then thread 0 propagates
-//      the band state to the successors (src/align.cpp:1516-1568).
+//      one comparison sweep over the predecessors; the left neighbour of a
+//      warp's first block comes from the scan summary), and the row's M/D
+//      blocks are written back to global memory, all 16-byte vector stores.
+// This kernel serves adaptive-band calls (-B, -S sub-windows); static-band
+// calls run k_plain_static (plain_static.cuh).
+//   4. with the adaptive band, a CTA argmax of M, then warp 0 propagates
+//      the band state to the successors (src/align.cpp:1516-1568), one lane
+//      per edge, and thread 0 prepares the next row's header.
 // After the last row thread 0 walks the records back from (n-1, m).
 #pragma once
 #include <climits>
@@ -71,53 +75,58 @@ __device__ __forceinline__ int64_t align16(int64_t x) { return (x + 15) & ~(int6
 
 struct RowShared {
     int32_t Bs, Be, bn, e0, d, status;
-    int64_t st, tb;
-    int64_t st_next, tb_next;  // next free row-store offset (spill area when ringed), next record offset
+    int64_t st, tb;  // the row's row-store offset and record offset
 };
 
-// A thread group that fills one alignment: the whole CTA (plain kernel) ...
+// Summary of one thread's block that lets another thread finalise the block's
+// last cell (finalize_last): its exclusive scan prefix without the chunk
+// carry, the max of its scan keys of cells 0..6, its H0[7].
+struct CellSum {
+    int32_t P, k06, h07;
+};
+
+// The CTA that fills one alignment. One barrier per chunk: every warp's
+// last lane publishes (warp-inclusive key max, its exclusive prefix, k06,
+// H0[7]) into a double-buffered array; after the barrier each warp forms the
+// cross-warp prefix itself, and lane 0 of every warp has the summary of its
+// left neighbour (the previous warp's last lane).
 template <int NT>
 struct CtaGroup {
     static constexpr int SIZE = NT;
     static constexpr int NW = NT / 32;
-    int32_t* s_scan;
-    int32_t* s_scan2;
-    int32_t* s_lastM;
-    int32_t* s_lastI;
+    int4* s_sum;  // [2][NW]
     unsigned long long* s_key;
-    RowShared* sr;
+    RowShared* sr;  // [2]: row i's header in sr[i & 1]
     __device__ __forceinline__ int tid() const { return threadIdx.x; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
-    // exclusive prefix max of per-thread aggregates; total = max over the group
-    __device__ __forceinline__ int32_t excl_max(int32_t agg, int32_t& total) const {
+    // P: exclusive prefix max of the aggregates (INT_MIN for thread 0), total:
+    // the max over the group, left: the summary of the thread to the left
+    // (lane 0 of warps >= 1 only), last: the summary of the group's last thread.
+    __device__ __forceinline__ void scan(int xp, int32_t agg, int32_t k06, int32_t h07, int32_t& P, int32_t& total,
+                                         CellSum& left, CellSum& last) const {
         const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         const int32_t incl = warp_incl_max(agg);
-        int32_t ex_w = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) ex_w = INT_MIN;
-        if (lane == 31) s_scan[wid] = incl;
+        int32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) ex = INT_MIN;
+        int4* buf = s_sum + xp * NW;
+        if (lane == 31) buf[wid] = make_int4(incl, ex, k06, h07);
         __syncthreads();
-        if (wid == 0) {
-            int32_t v = lane < NW ? s_scan[lane] : INT_MIN;
-            v = warp_incl_max(v);
-            if (lane < NW) s_scan2[lane] = v;
+        const int32_t wv = warp_incl_max(lane < NW ? buf[lane].x : INT_MIN);  // inclusive over warps
+        const int32_t wex1 = __shfl_sync(0xffffffffu, wv, wid >= 1 ? wid - 1 : 0);
+        const int32_t wex2 = __shfl_sync(0xffffffffu, wv, wid >= 2 ? wid - 2 : 0);
+        const int32_t wlast = __shfl_sync(0xffffffffu, wv, NW >= 2 ? NW - 2 : 0);
+        total = __shfl_sync(0xffffffffu, wv, NW - 1);
+        P = mx(ex, wid >= 1 ? wex1 : INT_MIN);
+        if (wid >= 1) {
+            const int4 L = buf[wid - 1];
+            left.P = mx(L.y, wid >= 2 ? wex2 : INT_MIN);
+            left.k06 = L.z;
+            left.h07 = L.w;
         }
-        __syncthreads();
-        total = s_scan2[NW - 1];
-        return mx(ex_w, wid > 0 ? s_scan2[wid - 1] : INT_MIN);
-    }
-    // left neighbour (M, I of the previous thread's last cell) and the values
-    // of the group's last thread (the carry into the next chunk)
-    __device__ __forceinline__ void edges(int32_t m7, int32_t i7, int32_t carryM, int32_t carryI, int32_t& Ml0,
-                                          int32_t& Il0, int32_t& nextM, int32_t& nextI) const {
-        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-        const int32_t upM = __shfl_up_sync(0xffffffffu, m7, 1);
-        const int32_t upI = __shfl_up_sync(0xffffffffu, i7, 1);
-        if (lane == 31) { s_lastM[wid] = m7; s_lastI[wid] = i7; }
-        __syncthreads();
-        Ml0 = lane > 0 ? upM : (wid > 0 ? s_lastM[wid - 1] : carryM);
-        Il0 = lane > 0 ? upI : (wid > 0 ? s_lastI[wid - 1] : carryI);
-        nextM = s_lastM[NW - 1];
-        nextI = s_lastI[NW - 1];
+        const int4 L = buf[NW - 1];
+        last.P = mx(L.y, NW >= 2 ? wlast : INT_MIN);
+        last.k06 = L.z;
+        last.h07 = L.w;
     }
     __device__ __forceinline__ unsigned long long max_u64(unsigned long long v) const {
         v = warp_max_u64(v);
@@ -127,43 +136,140 @@ struct CtaGroup {
         for (int w = 0; w < NW; w++) k = s_key[w] > k ? s_key[w] : k;
         return k;
     }
-    // thread 0 wrote *sr; make it visible to the group
-    __device__ __forceinline__ void publish() const { __syncthreads(); }
 };
 
-// ... or one warp (batched kernel: one warp per window)
-struct WarpGroup {
-    static constexpr int SIZE = 32;
-    RowShared* sr;
-    __device__ __forceinline__ int tid() const { return threadIdx.x & 31; }
-    __device__ __forceinline__ void sync() const { __syncwarp(); }
-    __device__ __forceinline__ int32_t excl_max(int32_t agg, int32_t& total) const {
-        const int lane = threadIdx.x & 31;
-        const int32_t incl = warp_incl_max(agg);
-        int32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0) ex = INT_MIN;
-        total = __shfl_sync(0xffffffffu, incl, 31);
-        return ex;
+// M and I of the last cell of the block summarised by `sm` (block index b),
+// given the chunk carry: row 0 has M = H0 and I = NEG_INF.
+__device__ __forceinline__ void summary_last(const Scoring& sc, int row, int b, const CellSum& sm, bool haveP,
+                                             int32_t carryP, int32_t& M7, int32_t& I7) {
+    if (row == 0) {
+        M7 = sm.h07;
+        I7 = NEG_INF;
+        return;
     }
-    __device__ __forceinline__ void edges(int32_t m7, int32_t i7, int32_t carryM, int32_t carryI, int32_t& Ml0,
-                                          int32_t& Il0, int32_t& nextM, int32_t& nextI) const {
-        const int lane = threadIdx.x & 31;
-        const int32_t upM = __shfl_up_sync(0xffffffffu, m7, 1);
-        const int32_t upI = __shfl_up_sync(0xffffffffu, i7, 1);
-        Ml0 = lane > 0 ? upM : carryM;
-        Il0 = lane > 0 ? upI : carryI;
-        nextM = __shfl_sync(0xffffffffu, m7, 31);
-        nextI = __shfl_sync(0xffffffffu, i7, 31);
-    }
-    __device__ __forceinline__ unsigned long long max_u64(unsigned long long v) const { return warp_max_u64(v); }
-    __device__ __forceinline__ void publish() const { __syncwarp(); }
-};
+    const int32_t P = haveP ? mx(sm.P, carryP) : sm.P;
+    finalize_last(sc, b * BLK, P, sm.k06, sm.h07, M7, I7);
+}
 
-// Fill all rows of one alignment with group G (see the file comment).
+// adaptive_update (dp_rowops.h, src/align.cpp:1516-1568) with the warp: the
+// predecessors' slope test and the successors' band updates run one lane per
+// edge (successors are distinct rows, so their updates do not collide); lane 0
+// settles row i's own state in between. Same results as the serial version.
+static __device__ void adaptive_update_warp(const DpArgs& a, int i, int Bs, int max_j, int lane) {
+    const int n = a.v.n;
+    int32_t* Mp = a.state + AB_MP * n;
+    int32_t* Sl = a.state + AB_SL * n;
+    int32_t* Pl = a.state + AB_PL * n;
+    int32_t* Pr = a.state + AB_PR * n;
+    int32_t* Ol = a.state + AB_OL * n;
+    int32_t* Or = a.state + AB_OR * n;
+    int32_t* Ow = a.state + AB_OW * n;
+    const int max_acj = Bs * BLK + max_j;
+    const bool base_match = (int)a.v.base[i] == (int)a.qs[max_acj + 1];  // cur.base == seq[max_acj]
+    int sl_best = INT_MIN, max_slp = 0;
+    bool is_match = false;
+    if (base_match) {
+        const int e0 = a.v.in_ptr[i], e1 = a.v.in_ptr[i + 1];
+        for (int e = e0 + lane; e < e1; e += 32) {
+            const int p = a.v.in_row[e];
+            const int slp = Sl[p];
+            max_slp = max(max_slp, slp);
+            if (Mp[p] + 1 == max_acj) {
+                is_match = true;
+                sl_best = max(sl_best, slp + 1);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
+            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
+        }
+        is_match = __any_sync(0xffffffffu, is_match);
+    }
+    int sl_i = 0, ow_i = 0, ol_i = 0, or_i = 0;
+    if (lane == 0) {
+        Mp[i] = max_acj;
+        sl_i = Sl[i];
+        ow_i = Ow[i];
+        ol_i = Ol[i];
+        or_i = Or[i];
+        if (is_match) sl_i = mx(sl_i, sl_best);
+        if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
+        if (sl_i >= 30) {
+            ol_i = or_i = max_acj - a.v.hq_loc[i];
+            ow_i = 0;
+        }
+        Sl[i] = sl_i;
+        Ow[i] = ow_i;
+        Ol[i] = ol_i;
+        Or[i] = or_i;
+    }
+    sl_i = __shfl_sync(0xffffffffu, sl_i, 0);
+    ow_i = __shfl_sync(0xffffffffu, ow_i, 0);
+    ol_i = __shfl_sync(0xffffffffu, ol_i, 0);
+    or_i = __shfl_sync(0xffffffffu, or_i, 0);
+    const int o0 = a.v.out_ptr[i], o1 = a.v.out_ptr[i + 1];
+    for (int e = o0 + lane; e < o1; e += 32) {
+        const int s = a.v.out_row[e];
+        if (sl_i >= 30) {
+            Ol[s] = ol_i;
+            Or[s] = or_i;
+        } else {
+            Ol[s] = mn(Ol[s], ol_i);
+            Or[s] = mx(Or[s], or_i);
+        }
+        Pl[s] = mn(Pl[s], max_acj);
+        Pr[s] = mx(Pr[s], max_acj + 1);
+        Ow[s] = ow_i ? mx(Ow[s], ow_i) : ow_i;
+    }
+    __syncwarp();
+}
+
+// Row header of row i (one thread): band, placement in the row store, record
+// offset and status; advances the bump offsets st_next / tb_next.
+__device__ __forceinline__ void row_header(const DpArgs& a, int i, int m, int64_t& st_next, int64_t& tb_next,
+                                           RowShared& sr) {
+    int Bs, Be;
+    row_band(a, i, m, Bs, Be);
+    if (i == 0) Bs = 0;
+    const int bn = Be - Bs - 1;
+    const int e0 = a.v.in_ptr[i];
+    const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
+    int st = ST_OK;
+    const int bpc = d >= 2 ? 4 : 1;
+    int64_t row_st = st_next;
+    bool linear = true;
+    if (a.ring_rows > 0) {
+        int maxs = i;
+        for (int e = a.v.out_ptr[i]; e < a.v.out_ptr[i + 1]; e++) maxs = max(maxs, a.v.out_row[e]);
+        const bool spill = (maxs - i >= a.ring_rows) || (bn > a.ring_blocks);
+        if (!spill) {
+            row_st = (int64_t)(i % a.ring_rows) * a.ring_blocks * 16;
+            linear = false;
+        }
+    }
+    if (bn < 0) st = ST_DEGENERATE;
+    else if (d > MAX_MULTI_PRED) st = ST_INDEGREE;
+    else if ((linear && row_st + (int64_t)bn * 16 > a.rs_cap) || tb_next + (int64_t)bn * BLK * bpc > a.tb_cap)
+        st = ST_OOM;
+    if (linear && st == ST_OK) st_next = row_st + (int64_t)bn * 16;
+    sr.Bs = Bs; sr.Be = Be; sr.bn = bn; sr.e0 = e0; sr.d = d; sr.status = st;
+    sr.st = row_st;
+    sr.tb = tb_next;
+    if (st == ST_OK) {
+        RowMeta rm;
+        rm.Bs = Bs; rm.Be = Be; rm.st = row_st; rm.tb = tb_next;
+        a.meta[i] = rm;
+        tb_next = align16(tb_next + (int64_t)bn * BLK * bpc);
+    }
+}
+
+// Fill all rows of one alignment with group G (see the file comment). Thread
+// 0 prepares row i+1's header right after row i's adaptive update, so one
+// barrier ends a row and publishes the next header (double-buffered).
 template <class G>
 __device__ void dp_fill(const G& g, const DpArgs& a) {
     constexpr int NT = G::SIZE;
-    RowShared& sr = *g.sr;
     const int tid = g.tid();
     const int n = a.v.n, m = a.qlen + 1;
     const bool adaptive = a.f > 0 && a.ab_band;
@@ -171,49 +277,15 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
 
     if (adaptive)
         for (int r = tid; r < n; r += NT) adaptive_init_entry(a, r, m);
-    if (tid == 0) {
-        sr.st_next = a.ring_rows > 0 ? (int64_t)a.ring_rows * a.ring_blocks * 16 : 0;
-        sr.tb_next = 0;
-    }
+    g.sync();
+    int64_t st_next = a.ring_rows > 0 ? (int64_t)a.ring_rows * a.ring_blocks * 16 : 0, tb_next = 0;  // thread 0
+    if (tid == 0) row_header(a, 0, m, st_next, tb_next, g.sr[0]);
     g.sync();
 
     int64_t cells = 0;
+    int xp = 0;  // parity of the group's scan buffer, flips every chunk
     for (int i = 0; i < n; i++) {
-        if (tid == 0) {
-            int Bs, Be;
-            row_band(a, i, m, Bs, Be);
-            if (i == 0) Bs = 0;
-            const int bn = Be - Bs - 1;
-            const int e0 = a.v.in_ptr[i];
-            const int d = i == 0 ? 0 : a.v.in_ptr[i + 1] - e0;
-            int st = ST_OK;
-            const int bpc = d >= 2 ? 4 : 1;
-            int64_t row_st = sr.st_next;
-            bool linear = true;
-            if (a.ring_rows > 0) {
-                int maxs = i;
-                for (int e = a.v.out_ptr[i]; e < a.v.out_ptr[i + 1]; e++) maxs = max(maxs, a.v.out_row[e]);
-                const bool spill = (maxs - i >= a.ring_rows) || (bn > a.ring_blocks);
-                if (!spill) {
-                    row_st = (int64_t)(i % a.ring_rows) * a.ring_blocks * 16;
-                    linear = false;
-                }
-            }
-            if (bn < 0) st = ST_DEGENERATE;
-            else if (d > MAX_MULTI_PRED) st = ST_INDEGREE;
-            else if ((linear && row_st + (int64_t)bn * 16 > a.rs_cap) || sr.tb_next + (int64_t)bn * BLK * bpc > a.tb_cap)
-                st = ST_OOM;
-            if (linear) sr.st_next = row_st + (int64_t)bn * 16;
-            sr.Bs = Bs; sr.Be = Be; sr.bn = bn; sr.e0 = e0; sr.d = d; sr.status = st;
-            sr.st = row_st;
-            sr.tb = sr.tb_next;
-            if (st == ST_OK) {
-                RowMeta rm;
-                rm.Bs = Bs; rm.Be = Be; rm.st = sr.st; rm.tb = sr.tb;
-                a.meta[i] = rm;
-            }
-        }
-        g.publish();
+        const RowShared& sr = g.sr[i & 1];
         const int Bs = sr.Bs, bn = sr.bn, e0 = sr.e0, d = sr.d;
         const int64_t rst = sr.st, rtb = sr.tb;
         if (sr.status != ST_OK) {
@@ -250,11 +322,12 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
                     const int pr = a.v.in_row[e];
                     const RowMeta pm = a.meta[pr];
                     const PredMask mk = pred_mask(B, pm.Bs, pm.Be);
+                    const int32_t* src = a.rs + pm.st;
                     int32_t Mb[BLK], Db[BLK];
                     int32_t mprev = NEG_INF;
-                    if (mk.prev_in) mprev = a.rs[pm.st + (int64_t)(B - 1 - pm.Bs) * 16 + 7];
+                    if (mk.prev_in) mprev = src[(int64_t)(B - 1 - pm.Bs) * 16 + 7];
                     if (mk.blk_in) {
-                        load_block16(a.rs + pm.st + (int64_t)(B - pm.Bs) * 16, Mb, Db);
+                        load_block16(src + (int64_t)(B - pm.Bs) * 16, Mb, Db);
                         pass1_pred(sc, mk, b == 0, a.v.in_base[e], Mb, Db, mprev, qc8, Mpre, Dv);
                     }
                     if (d == 1) {
@@ -267,15 +340,21 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
                     }
                 }
             }
-            int32_t agg = INT_MIN;
+            int32_t k06 = INT_MIN, agg = INT_MIN;
 #pragma unroll
             for (int l = 0; l < BLK; l++) {
                 H0[l] = mx(Mpre[l], Dv[l]);
-                if (act) agg = mx(agg, scan_key(H0[l], b * BLK + l, sc.e1));
+                if (act) {
+                    const int32_t key = scan_key(H0[l], b * BLK + l, sc.e1);
+                    if (l < BLK - 1) k06 = mx(k06, key);
+                    agg = mx(agg, key);
+                }
             }
             // group exclusive prefix max of the per-thread aggregates
-            int32_t chunk_total;
-            int32_t P = g.excl_max(agg, chunk_total);
+            int32_t chunk_total, P;
+            CellSum left, last;
+            g.scan(xp, agg, k06, H0[BLK - 1], P, chunk_total, left, last);
+            xp ^= 1;
             if (haveP) P = mx(P, carryP);
             if (act) {
                 if (i == 0) {
@@ -288,9 +367,21 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
 #pragma unroll
                 for (int l = 0; l < BLK; l++) { M[l] = NEG_INF; I[l] = NEG_INF; }
             }
-            // left neighbours of lane 0 of the block
-            int32_t Ml0, Il0, nextM, nextI;
-            g.edges(M[BLK - 1], I[BLK - 1], carryM, carryI, Ml0, Il0, nextM, nextI);
+            // left neighbour of the block's cell 0: the previous lane, the
+            // previous warp's last lane (from its summary), or the chunk carry
+            int32_t Ml0 = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
+            int32_t Il0 = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
+            if ((tid & 31) == 0) {
+                if (tid == 0) {
+                    Ml0 = carryM;
+                    Il0 = carryI;
+                } else {
+                    summary_last(sc, i, b - 1, left, haveP, carryP, Ml0, Il0);
+                }
+            }
+            if (c + 1 < nch) summary_last(sc, i, c * NT + NT - 1, last, haveP, carryP, carryM, carryI);
+            carryP = haveP ? mx(carryP, chunk_total) : chunk_total;
+            haveP = true;
             if (act) {
                 FlagAcc acc;
                 flag_acc_init(acc);
@@ -303,10 +394,11 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
                         const RowMeta pm = a.meta[pr];
                         const PredMask mk = pred_mask(B, pm.Bs, pm.Be);
                         if (!(mk.blk_in || mk.prev_in)) continue;
+                        const int32_t* src = a.rs + pm.st;
                         int32_t Mb[BLK], Db[BLK];
                         int32_t mprev = NEG_INF;
-                        if (mk.prev_in) mprev = a.rs[pm.st + (int64_t)(B - 1 - pm.Bs) * 16 + 7];
-                        if (mk.blk_in) load_block16(a.rs + pm.st + (int64_t)(B - pm.Bs) * 16, Mb, Db);
+                        if (mk.prev_in) mprev = src[(int64_t)(B - 1 - pm.Bs) * 16 + 7];
+                        if (mk.blk_in) load_block16(src + (int64_t)(B - pm.Bs) * 16, Mb, Db);
                         else {
 #pragma unroll
                             for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
@@ -346,28 +438,24 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
                     }
                 }
             }
-            carryP = haveP ? mx(carryP, chunk_total) : chunk_total;
-            haveP = true;
-            carryM = nextM;
-            carryI = nextI;
         }
         if (adaptive && i >= 1) {
             const unsigned long long k = g.max_u64(best);
-            if (tid == 0) {
+            if (tid < 32) {
                 const int max_j = bn > 0 ? (int)(0xffffffffu - (uint32_t)(k & 0xffffffffu)) : 0;
-                adaptive_update(a, i, Bs, max_j);
+                adaptive_update_warp(a, i, Bs, max_j, tid);
             }
         }
-        if (tid == 0) {
-            const int bpc = d >= 2 ? 4 : 1;
-            sr.tb_next = align16(rtb + (int64_t)bn * BLK * bpc);
-        }
+        if (tid == 0 && i + 1 < n) row_header(a, i + 1, m, st_next, tb_next, g.sr[(i + 1) & 1]);
         g.sync();
     }
     if (tid == 0) {
         const RowMeta last = a.meta[n - 1];
         const int jm = m - last.Bs * BLK;
-        a.out[1] = a.rs[last.st + (int64_t)(jm / BLK) * 16 + jm % BLK];
+        // column m lies in the last row's band (tlen[end] - tlen[end] = 0); the
+        // guard only keeps a malformed window from reading outside its row
+        const bool inb = jm >= 0 && jm / BLK < last.Be - last.Bs - 1;
+        a.out[1] = inb ? a.rs[last.st + (int64_t)(jm / BLK) * 16 + jm % BLK] : NEG_INF;
         a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
         a.out[0] = ST_OK;
     }
@@ -385,10 +473,10 @@ __global__ void __launch_bounds__(NT, 1) k_plain(const DpArgs* __restrict__ jobs
         return;
     }
     constexpr int NW = NT / 32;
-    __shared__ int32_t s_scan[NW], s_scan2[NW], s_lastM[NW], s_lastI[NW];
+    __shared__ int4 s_sum[2 * NW];
     __shared__ unsigned long long s_key[NW];
-    __shared__ RowShared sr;
-    CtaGroup<NT> g{s_scan, s_scan2, s_lastM, s_lastI, s_key, &sr};
+    __shared__ RowShared sr[2];
+    CtaGroup<NT> g{s_sum, s_key, sr};
     dp_fill(g, a);
     __syncthreads();
     if (threadIdx.x == 0 && a.out[0] == ST_OK) {

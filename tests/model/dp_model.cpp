@@ -149,6 +149,12 @@ struct ModelEngine : DpEngine {
                     for (int l = 0; l < BLK; l++) { M[l] = H0[b * BLK + l]; I[l] = NEG_INF; }
                 } else {
                     finalize_block(sc, b * BLK, P, &H0[b * BLK], M, I);
+                    // the static-band plain kernel derives a warp's left neighbour
+                    // from the scan summary alone; it must equal the full block
+                    int32_t k06 = scan_key(H0[b * BLK], b * BLK, sc.e1), M7, I7;
+                    for (int l = 1; l < BLK - 1; l++) k06 = mx(k06, scan_key(H0[b * BLK + l], b * BLK + l, sc.e1));
+                    finalize_last(sc, b * BLK, P, k06, H0[b * BLK + BLK - 1], M7, I7);
+                    if (M7 != M[BLK - 1] || I7 != I[BLK - 1]) { a.out[0] = ST_BAD_ARG; return; }
                 }
                 for (int l = 0; l < BLK; l++) {
                     int32_t key = scan_key(H0[b * BLK + l], b * BLK + l, sc.e1);

@@ -50,6 +50,25 @@ def edge_reads():
     }
 
 
+def long_indel_reads():
+    """Reads with 45-80 bp insertions and deletions against one template: the
+    graph gets rows whose successor lies 45+ rows ahead in rank order, so the
+    kernels' row rings must hand those rows to the global row store."""
+    rng = np.random.default_rng(31)
+    t = synth.to_ascii(synth.random_root(rng, 1500))
+    ins = [synth.to_ascii(synth.random_root(rng, k)) for k in (60, 45, 80)]
+    sub = bytearray(t)
+    for x in rng.choice(len(sub), 15, replace=False):
+        sub[x] = b"ACGT"[(b"ACGT".index(sub[x]) + 1) % 4]
+    return [t,
+            t[:400] + ins[0] + t[400:900] + t[960:],
+            t[:400] + ins[0] + t[400:],
+            t[:900] + t[960:],
+            bytes(sub[:1200]) + ins[1] + bytes(sub[1200:]),
+            t[:250] + ins[2] + t[250:700] + t[780:],
+            t]
+
+
 def cases():
     out = []
     out.append(("cons_small", synth.single_graph_consensus(seed=11, nseq=6, length=800), [], True))
@@ -72,6 +91,11 @@ def cases():
         out.append((name + "_adaptive", reads, ["-B"], False))
         out.append((name + "_msa", reads, ["-r", "1"], False))
         out.append((name + "_gfa", reads, ["-r", "2"], False))
+    li = long_indel_reads()
+    out.append(("long_indel", li, [], True))
+    out.append(("long_indel_fullband", li, ["-f", "0"], True))
+    out.append(("long_indel_adaptive", li, ["-B"], True))
+    out.append(("long_indel_msa", li, ["-r", "1"], False))
     seed_in = synth.single_graph_msa(seed=17, nseq=10, length=3000)
     out.append(("seeded_msa", seed_in, ["-S", "-r", "1"], False))
     out.append(("seeded_cons", seed_in, ["-S"], False))

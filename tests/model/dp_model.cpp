@@ -1,6 +1,6 @@
 // dp_model.cpp - TEST-ONLY sequential model of the CUDA DP kernels.
 //
-// It runs exactly the per-block steps of plain.cu (pass 1 over predecessors,
+// It runs exactly the per-block steps of plain.cuh (pass 1 over predecessors,
 // prefix-max scan, finalisation, backtrack records, row store layout, the
 // record-driven backtrack) one block at a time on the CPU, using the same
 // dp_core.h / dp_rowops.h functions the kernels use. The tests compare it with
@@ -149,7 +149,7 @@ struct ModelEngine : DpEngine {
                     for (int l = 0; l < BLK; l++) { M[l] = H0[b * BLK + l]; I[l] = NEG_INF; }
                 } else {
                     finalize_block(sc, b * BLK, P, &H0[b * BLK], M, I);
-                    // the static-band plain kernel derives a warp's left neighbour
+                    // the single-alignment kernels derive a warp's left neighbour
                     // from the scan summary alone; it must equal the full block
                     int32_t k06 = scan_key(H0[b * BLK], b * BLK, sc.e1), M7, I7;
                     for (int l = 1; l < BLK - 1; l++) k06 = mx(k06, scan_key(H0[b * BLK + l], b * BLK + l, sc.e1));
@@ -246,4 +246,37 @@ int model_run_gfa(int nseq, const char* const* seqs, const int* lens, const int*
 }
 
 void model_free(void* p) { free(p); }
+
+// finalize_last against finalize_block on random blocks: H0 values from the
+// whole int32 range near NEG_INF up to large scores, random prefixes P and
+// block positions, several scorings. Returns the number of mismatches.
+int model_check_finalize_last(uint64_t seed, int iters) {
+    uint64_t x = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto rnd = [&x]() {
+        x ^= x << 13; x ^= x >> 7; x ^= x << 17;
+        return x;
+    };
+    const int32_t pool[] = {NEG_INF, NEG_INF + 1, NEG_INF + 7, -1000000, -5, 0, 3, 1000000, 0x3f3f3f3f};
+    int bad = 0;
+    for (int it = 0; it < iters; it++) {
+        Scoring sc;
+        sc.match = (int32_t)(rnd() % 5);
+        sc.mismatch = -(int32_t)(rnd() % 7);
+        const int32_t e1 = -(int32_t)(1 + rnd() % 4);
+        sc.e1 = e1;
+        sc.o1 = e1 - (int32_t)(rnd() % 8);  // o1 <= e1, as the prefix-max form requires
+        const int j0 = (int)(rnd() % 3 == 0 ? 0 : (rnd() % 4096) * BLK);
+        int32_t H0[BLK];
+        for (int l = 0; l < BLK; l++)
+            H0[l] = rnd() % 3 == 0 ? pool[rnd() % 9] : (int32_t)(rnd() % 4000000) - 2000000;
+        const int32_t P = rnd() % 4 == 0 ? pool[rnd() % 9] : (int32_t)(rnd() % 4000000) - 2000000;
+        int32_t M[BLK], I[BLK], M7, I7;
+        finalize_block(sc, j0, P, H0, M, I);
+        int32_t k06 = scan_key(H0[0], j0, sc.e1);
+        for (int l = 1; l < BLK - 1; l++) k06 = mx(k06, scan_key(H0[l], j0 + l, sc.e1));
+        finalize_last(sc, j0, P, k06, H0[BLK - 1], M7, I7);
+        if (M7 != M[BLK - 1] || I7 != I[BLK - 1]) bad++;
+    }
+    return bad;
+}
 }

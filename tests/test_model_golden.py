@@ -44,7 +44,17 @@ def model():
                                   ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_void_p),
                                   ctypes.POINTER(ctypes.c_int), ctypes.c_int]
     lib.model_free.argtypes = [ctypes.c_void_p]
+    lib.model_check_finalize_last.restype = ctypes.c_int
+    lib.model_check_finalize_last.argtypes = [ctypes.c_uint64, ctypes.c_int]
     return lib
+
+
+def test_finalize_last_matches_finalize_block(model):
+    """The single-alignment kernels take a warp's left neighbour (M, I of the
+    previous block's last cell) from the scan summary alone (finalize_last);
+    it must equal the full block finalisation for any values, wrap-around
+    near NEG_INF included."""
+    assert model.model_check_finalize_last(2024, 200000) == 0
 
 
 def opts_to_params(opts):

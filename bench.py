@@ -404,7 +404,7 @@ def ours(args, world, rank, local, D):
             same += txt == b">consensus sequence\n" + cons[w] + b"\n"
         dt = time.perf_counter() - t0
         line["plain_kernel"] = {"value": n / dt, "unit": "windows/s", "windows": n, "identical_consensus": same,
-                                "path": "poa_run: one CTA per poa() call (k_plain), graph fused on the host",
+                                "path": "poa_run: one CTA per poa() call (k_plain_static for the static band, k_plain for -B), graph fused on the host",
                                 "speedup": value / (n / dt)}
     if rank == 0 and world == 1 and not args.no_cpu:
         binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN

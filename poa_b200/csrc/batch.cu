@@ -1144,77 +1144,6 @@ __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__
 // (src/align.cpp:1516-1568). out[4] / out[5]: record bytes and spilled
 // row-store entries used.
 constexpr int DYN_STAGE_EDGES = 128;
-// prefetched adaptive-update inputs (int32 slots): predecessors' Sl, Mp; successors'
-// Ol, Or, Pl, Pr, Ow and row index; the row's own Sl, Ow, Ol, Or
-constexpr int UPD_PSL = 0, UPD_PMP = 32, UPD_SOL = 64, UPD_SOR = 96, UPD_SPL = 128, UPD_SPR = 160, UPD_SOW = 192,
-              UPD_SROW = 224, UPD_OWN = 256, UPD_INTS = 260, UPD_BYTES = 1088;
-
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit_all() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// adaptive_update_warp with its inputs already in shared memory (copied with
-// cp.async when the row started; nothing else writes them in between: the
-// predecessors are finished, and only this row's update changes its own and
-// its successors' state). Needs d <= 32 predecessors and ns <= 32 successors.
-__device__ void adaptive_update_pf(const DpArgs& a, int i, int Bs, int max_j, int lane, const int32_t* upd, int d,
-                                   int ns, int base_i, int hql, const uint8_t* __restrict__ qf) {
-    const int n = a.v.n;
-    int32_t* Mp = a.state + AB_MP * n;
-    int32_t* Sl = a.state + AB_SL * n;
-    int32_t* Pl = a.state + AB_PL * n;
-    int32_t* Pr = a.state + AB_PR * n;
-    int32_t* Ol = a.state + AB_OL * n;
-    int32_t* Or = a.state + AB_OR * n;
-    int32_t* Ow = a.state + AB_OW * n;
-    const int max_acj = Bs * BLK + max_j;
-    const bool base_match = base_i == (int)qf[max_acj + 1];  // cur.base == seq[max_acj]
-    int sl_best = INT_MIN, max_slp = 0;
-    bool is_match = false;
-    if (base_match) {
-        if (lane < d) {
-            const int slp = upd[UPD_PSL + lane];
-            max_slp = slp;
-            if (upd[UPD_PMP + lane] + 1 == max_acj) {
-                is_match = true;
-                sl_best = slp + 1;
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
-            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
-        }
-        is_match = __any_sync(0xffffffffu, is_match);
-    }
-    int sl_i = upd[UPD_OWN + 0], ow_i = upd[UPD_OWN + 1], ol_i = upd[UPD_OWN + 2], or_i = upd[UPD_OWN + 3];
-    if (is_match) sl_i = mx(sl_i, sl_best);
-    if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
-    if (sl_i >= 30) {
-        ol_i = or_i = max_acj - hql;
-        ow_i = 0;
-    }
-    if (lane == 0) {
-        Mp[i] = max_acj;
-        Sl[i] = sl_i;
-        Ow[i] = ow_i;
-        Ol[i] = ol_i;
-        Or[i] = or_i;
-    }
-    if (lane < ns) {
-        const int s = upd[UPD_SROW + lane];
-        Ol[s] = sl_i >= 30 ? ol_i : mn(upd[UPD_SOL + lane], ol_i);
-        Or[s] = sl_i >= 30 ? or_i : mx(upd[UPD_SOR + lane], or_i);
-        Pl[s] = mn(upd[UPD_SPL + lane], max_acj);
-        Pr[s] = mx(upd[UPD_SPR + lane], max_acj + 1);
-        Ow[s] = ow_i ? mx(upd[UPD_SOW + lane], ow_i) : ow_i;
-    }
-    __syncwarp();
-}
-
 __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const int32_t* __restrict__ vmaxs,
                                  const uint8_t* __restrict__ qsm, int4* sed, int32_t* upd, int lane) {
     const int n = a.v.n, m = a.qlen + 1;

@@ -68,7 +68,8 @@ __global__ void __launch_bounds__(NT, 1) k_plain_noalloc(DpArgs a, const uint8_t
     __shared__ int4 s_sum[2 * NW];
     __shared__ unsigned long long s_key[NW];
     __shared__ RowShared sr[2];
-    CtaGroup<NT> g{s_sum, s_key, sr};
+    __shared__ int32_t s_upd[UPD_INTS];
+    CtaGroup<NT> g{s_sum, s_key, sr, s_upd};
     dp_fill(g, a);
     __syncthreads();
     if (threadIdx.x == 0 && a.out[0] == ST_OK) {

@@ -13,12 +13,13 @@
 //      one comparison sweep over the predecessors; the left neighbour of a
 //      warp's first block comes from the scan summary), and the row's M/D
 //      blocks are written back to global memory, all 16-byte vector stores.
-// This kernel serves adaptive-band calls (-B, -S sub-windows); static-band
-// calls run k_plain_static (plain_static.cuh).
 //   4. with the adaptive band, a CTA argmax of M, then warp 0 propagates
 //      the band state to the successors (src/align.cpp:1516-1568), one lane
-//      per edge, and thread 0 prepares the next row's header.
+//      per edge, from inputs it copied with cp.async when the row started;
+//      thread 0 then prepares the next row's header.
 // After the last row thread 0 walks the records back from (n-1, m).
+// This kernel serves adaptive-band calls (-B, -S sub-windows); static-band
+// calls run k_plain_static (plain_static.cuh).
 #pragma once
 #include <climits>
 
@@ -97,6 +98,7 @@ struct CtaGroup {
     int4* s_sum;  // [2][NW]
     unsigned long long* s_key;
     RowShared* sr;  // [2]: row i's header in sr[i & 1]
+    int32_t* upd;   // [UPD_INTS]: the adaptive update's inputs (adaptive band only)
     __device__ __forceinline__ int tid() const { return threadIdx.x; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
     // P: exclusive prefix max of the aggregates (INT_MIN for thread 0), total:
@@ -225,6 +227,77 @@ static __device__ void adaptive_update_warp(const DpArgs& a, int i, int Bs, int 
     __syncwarp();
 }
 
+// prefetched adaptive-update inputs (int32 slots): predecessors' Sl, Mp; successors'
+// Ol, Or, Pl, Pr, Ow and row index; the row's own Sl, Ow, Ol, Or
+constexpr int UPD_PSL = 0, UPD_PMP = 32, UPD_SOL = 64, UPD_SOR = 96, UPD_SPL = 128, UPD_SPR = 160, UPD_SOW = 192,
+              UPD_SROW = 224, UPD_OWN = 256, UPD_INTS = 260, UPD_BYTES = 1088;
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_all() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// adaptive_update_warp with its inputs already in shared memory (copied with
+// cp.async when the row started; nothing else writes them in between: the
+// predecessors are finished, and only this row's update changes its own and
+// its successors' state). Needs d <= 32 predecessors and ns <= 32 successors.
+static __device__ void adaptive_update_pf(const DpArgs& a, int i, int Bs, int max_j, int lane, const int32_t* upd, int d,
+                                   int ns, int base_i, int hql, const uint8_t* __restrict__ qf) {
+    const int n = a.v.n;
+    int32_t* Mp = a.state + AB_MP * n;
+    int32_t* Sl = a.state + AB_SL * n;
+    int32_t* Pl = a.state + AB_PL * n;
+    int32_t* Pr = a.state + AB_PR * n;
+    int32_t* Ol = a.state + AB_OL * n;
+    int32_t* Or = a.state + AB_OR * n;
+    int32_t* Ow = a.state + AB_OW * n;
+    const int max_acj = Bs * BLK + max_j;
+    const bool base_match = base_i == (int)qf[max_acj + 1];  // cur.base == seq[max_acj]
+    int sl_best = INT_MIN, max_slp = 0;
+    bool is_match = false;
+    if (base_match) {
+        if (lane < d) {
+            const int slp = upd[UPD_PSL + lane];
+            max_slp = slp;
+            if (upd[UPD_PMP + lane] + 1 == max_acj) {
+                is_match = true;
+                sl_best = slp + 1;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            max_slp = max(max_slp, __shfl_xor_sync(0xffffffffu, max_slp, o));
+            sl_best = max(sl_best, __shfl_xor_sync(0xffffffffu, sl_best, o));
+        }
+        is_match = __any_sync(0xffffffffu, is_match);
+    }
+    int sl_i = upd[UPD_OWN + 0], ow_i = upd[UPD_OWN + 1], ol_i = upd[UPD_OWN + 2], or_i = upd[UPD_OWN + 3];
+    if (is_match) sl_i = mx(sl_i, sl_best);
+    if (!is_match && max_slp < 30) ow_i = mn(ow_i + max_slp + 1, 5 * a.w);
+    if (sl_i >= 30) {
+        ol_i = or_i = max_acj - hql;
+        ow_i = 0;
+    }
+    if (lane == 0) {
+        Mp[i] = max_acj;
+        Sl[i] = sl_i;
+        Ow[i] = ow_i;
+        Ol[i] = ol_i;
+        Or[i] = or_i;
+    }
+    if (lane < ns) {
+        const int s = upd[UPD_SROW + lane];
+        Ol[s] = sl_i >= 30 ? ol_i : mn(upd[UPD_SOL + lane], ol_i);
+        Or[s] = sl_i >= 30 ? or_i : mx(upd[UPD_SOR + lane], or_i);
+        Pl[s] = mn(upd[UPD_SPL + lane], max_acj);
+        Pr[s] = mx(upd[UPD_SPR + lane], max_acj + 1);
+        Ow[s] = ow_i ? mx(upd[UPD_SOW + lane], ow_i) : ow_i;
+    }
+    __syncwarp();
+}
+
 // Row header of row i (one thread): band, placement in the row store, record
 // offset and status; advances the bump offsets st_next / tb_next.
 __device__ __forceinline__ void row_header(const DpArgs& a, int i, int m, int64_t& st_next, int64_t& tb_next,
@@ -291,6 +364,40 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
         if (sr.status != ST_OK) {
             if (tid == 0) a.out[0] = sr.status;
             return;
+        }
+        // the adaptive update's inputs, copied by warp 0 while the row is filled
+        // (nothing else writes them before the update: the predecessors are done
+        // and only this row's update changes its own and its successors' state)
+        int ns = 0, base_i = 0, hql = 0;
+        bool pf = false;
+        if (adaptive && i >= 1 && tid < 32) {
+            const int o0 = a.v.out_ptr[i];
+            ns = a.v.out_ptr[i + 1] - o0;
+            pf = d <= 32 && ns <= 32;
+            if (pf) {
+                base_i = a.v.base[i];
+                hql = a.v.hq_loc[i];
+                const int32_t* st_ = a.state;
+                if (tid < ns) {
+                    const int s = a.v.out_row[o0 + tid];
+                    g.upd[UPD_SROW + tid] = s;
+                    cp_async4(g.upd + UPD_SOL + tid, st_ + AB_OL * n + s);
+                    cp_async4(g.upd + UPD_SOR + tid, st_ + AB_OR * n + s);
+                    cp_async4(g.upd + UPD_SPL + tid, st_ + AB_PL * n + s);
+                    cp_async4(g.upd + UPD_SPR + tid, st_ + AB_PR * n + s);
+                    cp_async4(g.upd + UPD_SOW + tid, st_ + AB_OW * n + s);
+                }
+                if (tid < 4) {
+                    const int arr = tid == 0 ? AB_SL : tid == 1 ? AB_OW : tid == 2 ? AB_OL : AB_OR;
+                    cp_async4(g.upd + UPD_OWN + tid, st_ + arr * n + i);
+                }
+                if (tid < d) {
+                    const int p = a.v.in_row[e0 + tid];
+                    cp_async4(g.upd + UPD_PSL + tid, st_ + AB_SL * n + p);
+                    cp_async4(g.upd + UPD_PMP + tid, st_ + AB_MP * n + p);
+                }
+                cp_async_commit_all();
+            }
         }
         cells += (int64_t)bn * BLK;
         const int nch = (bn + NT - 1) / NT;
@@ -443,7 +550,13 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
             const unsigned long long k = g.max_u64(best);
             if (tid < 32) {
                 const int max_j = bn > 0 ? (int)(0xffffffffu - (uint32_t)(k & 0xffffffffu)) : 0;
-                adaptive_update_warp(a, i, Bs, max_j, tid);
+                if (pf) {
+                    cp_async_wait_all();
+                    __syncwarp();
+                    adaptive_update_pf(a, i, Bs, max_j, tid, g.upd, d, ns, base_i, hql, a.qs);
+                } else {
+                    adaptive_update_warp(a, i, Bs, max_j, tid);
+                }
             }
         }
         if (tid == 0 && i + 1 < n) row_header(a, i + 1, m, st_next, tb_next, g.sr[(i + 1) & 1]);
@@ -476,7 +589,8 @@ __global__ void __launch_bounds__(NT, 1) k_plain(const DpArgs* __restrict__ jobs
     __shared__ int4 s_sum[2 * NW];
     __shared__ unsigned long long s_key[NW];
     __shared__ RowShared sr[2];
-    CtaGroup<NT> g{s_sum, s_key, sr};
+    __shared__ int32_t s_upd[UPD_INTS];
+    CtaGroup<NT> g{s_sum, s_key, sr, s_upd};
     dp_fill(g, a);
     __syncthreads();
     if (threadIdx.x == 0 && a.out[0] == ST_OK) {

@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(NT, 1) k_plain_static(const DpArgs* __restrict
     }
     const int R = a.ring_rows, RB = a.ring_blocks;
     const Scoring sc = a.sc;
-    const CtaGroup<NT> g{s_sum, nullptr, nullptr};  // scan only
+    const CtaGroup<NT> g{s_sum, nullptr, nullptr, nullptr};  // scan only
 
     // ---- rows: band, placement, record offset (src/align.cpp:1382-1391) ----
     int64_t st_run = 0, tb_run = 0;

@@ -574,7 +574,104 @@ __device__ void dp_fill(const G& g, const DpArgs& a) {
     }
 }
 
-// one CTA per job: fill every row, then thread 0 backtracks
+// Backtrack by one warp: all 32 lanes call it with the same arguments and
+// take the same steps as backtrack_records (dp_rowops.h, src/align.cpp:
+// 1572-1736), with the same results; lane 0 writes the moves. What differs is
+// how the data arrive: the lanes fetch ahead along the diagonal, lane k
+// loading the row header, record, query code and first predecessor edge of
+// cell (i0 - k, acj0 - k), so a run of diagonal moves to the previous row
+// costs no further memory round trip. Any other move starts a new fetch at
+// the cell it reaches.
+static __device__ __noinline__ int32_t backtrack_warp(const DpArgs& a, int m, int lane, int32_t& nmoves) {
+    int i = a.v.n - 1, acj = m, op = ALL_OP;
+    int32_t nm = 0;
+    int i0 = -1, a0 = 0;  // origin of the fetched diagonal
+    int f_Bs = 0, f_Be = 0, f_e0 = 0, f_d = 0, f_qc = 4, f_row0 = 0, f_base0 = 0;
+    uint32_t f_rec = 0;
+    while (i > 0 || acj > 0) {
+        int k = i0 - i;
+        if (!(i0 >= 0 && k >= 0 && k < 32 && a0 - acj == k)) {
+            i0 = i;
+            a0 = acj;
+            k = 0;
+            const int r = i0 - lane, c = a0 - lane;
+            f_Bs = f_Be = f_e0 = f_d = f_row0 = f_base0 = 0;
+            f_qc = 4;
+            f_rec = 0;
+            if (r >= 0 && c >= 0) {
+                const RowMeta rm = a.meta[r];
+                f_Bs = rm.Bs;
+                f_Be = rm.Be;
+                f_e0 = a.v.in_ptr[r];
+                f_d = a.v.in_ptr[r + 1] - f_e0;
+                f_qc = c > 0 ? a.qs[c] : 4;
+                const int j = c - rm.Bs * BLK, bn = rm.Be - rm.Bs - 1;
+                if (c <= (rm.Be - 1) * BLK && c >= rm.Bs * BLK && j < bn * BLK)
+                    f_rec = f_d >= 2 ? *reinterpret_cast<const uint32_t*>(a.tb + rm.tb + (int64_t)j * 4)
+                                     : (uint32_t)a.tb[rm.tb + j];
+                if (f_d >= 1) {
+                    f_row0 = a.v.in_row[f_e0];
+                    f_base0 = a.v.in_base[f_e0];
+                }
+            }
+        }
+        const int Bs = __shfl_sync(0xffffffffu, f_Bs, k), Be = __shfl_sync(0xffffffffu, f_Be, k);
+        const int e0 = __shfl_sync(0xffffffffu, f_e0, k), d = __shfl_sync(0xffffffffu, f_d, k);
+        const int qck = __shfl_sync(0xffffffffu, f_qc, k);
+        const int row0 = __shfl_sync(0xffffffffu, f_row0, k), base0 = __shfl_sync(0xffffffffu, f_base0, k);
+        const uint32_t raw = __shfl_sync(0xffffffffu, f_rec, k);
+        if (acj > (Be - 1) * BLK || acj < Bs * BLK) { nmoves = nm; return ST_BAND_ESCAPE; }
+        const int j = acj - Bs * BLK;
+        const int bn = Be - Bs - 1;
+        if (j >= bn * BLK) { nmoves = nm; return ST_BT_FAIL; }
+        const Rec r = d >= 2 ? decode_wide(raw) : decode_small((uint8_t)raw);
+        if (nm + 1 > a.moves_cap) { nmoves = nm; return ST_OOM; }
+        const int qc = acj > 0 ? qck : 4;
+        if ((op & M_OP) && acj > 0 && r.m1 >= 0) {
+            const bool first = r.m1 == 0 && d >= 1;
+            const int p = first ? row0 : a.v.in_row[e0 + r.m1];
+            const int pb = first ? base0 : (int)a.v.in_base[e0 + r.m1];
+            if (lane == 0) a.moves[nm] = mv_pack(pb == qc ? MV_MATCH : MV_MISMATCH, p, qc);
+            nm++;
+            op = ALL_OP; i = p; acj--;
+            continue;
+        }
+        if ((op & D_OP) && (op == D_OP || r.eqMD) && r.dpos >= 0) {
+            i = r.dpos == 0 && d >= 1 ? row0 : a.v.in_row[e0 + r.dpos];
+            op = r.dext ? D_OP : (M_OP | I_OP);
+            continue;
+        }
+        if ((op & I_OP) && acj > 0 && j >= 1 && (op == I_OP || r.eqMI)) {
+            if (r.iopen) {
+                if (lane == 0) a.moves[nm] = mv_pack(MV_INSERT, 0, qc);
+                nm++;
+                op = M_OP | D_OP; acj--;
+                continue;
+            }
+            if (r.iext) {
+                if (lane == 0) a.moves[nm] = mv_pack(MV_INSERT, 0, qc);
+                nm++;
+                op = I_OP; acj--;
+                continue;
+            }
+        }
+        if ((op & M_OP) && acj > 0 && r.m4 >= 0) {
+            const bool first = r.m4 == 0 && d >= 1;
+            const int p = first ? row0 : a.v.in_row[e0 + r.m4];
+            const int pb = first ? base0 : (int)a.v.in_base[e0 + r.m4];
+            if (lane == 0) a.moves[nm] = mv_pack(pb == qc ? MV_MATCH : MV_MISMATCH, p, qc);
+            nm++;
+            op = ALL_OP; i = p; acj--;
+            continue;
+        }
+        nmoves = nm;
+        return ST_BT_FAIL;
+    }
+    nmoves = nm;
+    return ST_OK;
+}
+
+// one CTA per job: fill every row, then warp 0 backtracks
 template <int NT>
 __global__ void __launch_bounds__(NT, 1) k_plain(const DpArgs* __restrict__ jobs) {
     __shared__ DpArgs sa;
@@ -593,10 +690,13 @@ __global__ void __launch_bounds__(NT, 1) k_plain(const DpArgs* __restrict__ jobs
     CtaGroup<NT> g{s_sum, s_key, sr, s_upd};
     dp_fill(g, a);
     __syncthreads();
-    if (threadIdx.x == 0 && a.out[0] == ST_OK) {
+    if (threadIdx.x < 32 && a.out[0] == ST_OK) {
         int32_t nm = 0;
-        a.out[0] = backtrack_records(a, a.qlen + 1, nm);
-        a.out[2] = nm;
+        const int32_t st = backtrack_warp(a, a.qlen + 1, threadIdx.x, nm);
+        if (threadIdx.x == 0) {
+            a.out[0] = st;
+            a.out[2] = nm;
+        }
     }
 }
 

@@ -18,7 +18,8 @@
 // i % ring_rows); a row with an in-window successor ring_rows or more rows
 // ahead, or wider than the ring, goes to the global row store instead. A ring
 // row's RowMeta.st holds ~(its offset in the ring), a global row's st >= 0.
-// Results are identical to k_plain's: same per-block functions, same records.
+// Results are identical to k_plain's: same per-block functions, same records,
+// and the same warp backtrack (backtrack_warp).
 #pragma once
 #include "plain.cuh"
 
@@ -286,17 +287,20 @@ __global__ void __launch_bounds__(NT, 1) k_plain_static(const DpArgs* __restrict
         prevm = cur;
         __syncthreads();  // barrier 2: the row's M/D before the next row reads them
     }
-    if (tid == 0) {
-        const RowMeta last = prevm;
-        const int jm = m - last.Bs * BLK;
-        // column m lies in the last row's band (tlen[end] - tlen[end] = 0); the
-        // guard only keeps a malformed window from reading outside its row
-        const bool inb = jm >= 0 && jm / BLK < last.Be - last.Bs - 1;
-        a.out[1] = inb ? row_src(ring, a.rs, last.st)[(int64_t)(jm / BLK) * 16 + jm % BLK] : NEG_INF;
-        a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+    if (tid < 32) {  // warp 0: score, then the backtrack
         int32_t nm = 0;
-        a.out[0] = backtrack_records(a, m, nm);
-        a.out[2] = nm;
+        const int32_t st = backtrack_warp(a, m, tid, nm);
+        if (tid == 0) {
+            const RowMeta last = prevm;
+            const int jm = m - last.Bs * BLK;
+            // column m lies in the last row's band (tlen[end] - tlen[end] = 0); the
+            // guard only keeps a malformed window from reading outside its row
+            const bool inb = jm >= 0 && jm / BLK < last.Be - last.Bs - 1;
+            a.out[1] = inb ? row_src(ring, a.rs, last.st)[(int64_t)(jm / BLK) * 16 + jm % BLK] : NEG_INF;
+            a.out[3] = (int32_t)(cells > INT_MAX ? INT_MAX : cells);
+            a.out[0] = st;
+            a.out[2] = nm;
+        }
     }
 }
 

@@ -56,15 +56,15 @@ struct ModelEngine : DpEngine {
         a.moves = moves.data();
         a.moves_cap = (int32_t)moves.size();
         a.out = out;
-        // generous capacity: every row at full width
+        // a small ring (4 rows) exercises the ring/spill placement of the kernels;
+        // generous capacity: the ring plus every row at full width
         int64_t full_blocks = (int64_t)(m / BLK + 2);
-        rs.assign((size_t)(n * full_blocks * 16 + 16), 0);
+        a.ring_rows = 4;
+        a.ring_blocks = (int32_t)std::min<int64_t>(full_blocks, 24);
+        rs.assign((size_t)((int64_t)a.ring_rows * a.ring_blocks * 16 + n * full_blocks * 16 + 16), 0);
         tb.assign((size_t)(n * (full_blocks * BLK * 4 + 16) + 16), 0);
         a.rs = rs.data();
         a.rs_cap = (int64_t)rs.size();
-        // a small ring (4 rows) exercises the ring/spill placement of the kernels
-        a.ring_rows = 4;
-        a.ring_blocks = (int32_t)std::min<int64_t>(full_blocks, 24);
         a.tb = tb.data();
         a.tb_cap = (int64_t)tb.size();
         fill(a, m);

@@ -181,10 +181,13 @@ int poa_batch_read_stats(poa_ctx* ctx, int32_t* out, int64_t cap);
  * loads the library until the process exits.
  *
  * Limit: the window must fit that array at its worst case (every row at the
- * full band width): roughly n_rows * (qlen/8 + 2) * 96 bytes plus
- * n_rows * 48 bytes must stay under POA_NOALLOC_SCRATCH_BYTES (64 MiB), e.g.
- * 1,500 rows with a 700 bp query, or 400 rows with a 10 kb query. Larger
- * windows are rejected with POA_OOM before anything is launched.
+ * full band width): about n_rows * (96 * ((qlen + 1) / 8 + 1) + 68) bytes,
+ * plus the query, must stay under POA_NOALLOC_SCRATCH_BYTES (64 MiB). That
+ * is up to about 7,800 rows with a 700 bp query, or about 550 rows with a
+ * 10 kb query. Larger windows are rejected with POA_OOM before anything is
+ * launched; impossible sizes (negative, or a query whose buffer alone
+ * exceeds the array) are rejected the same way, with no arithmetic that can
+ * wrap. On a failed alignment result_dev[1..3] are 0.
  *
  * w: the window's rows (ranks beg..end), laid out like the rows poa_align
  * builds: CSR predecessor lists in in-list order (predecessor row, its
@@ -200,7 +203,9 @@ int poa_batch_read_stats(poa_ctx* ctx, int32_t* out, int64_t cap);
  *
  * The first call on each device looks up the scratch array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. Every call reuses the same array: calls whose
+ * before any stream capture. The address is kept for the life of the
+ * process: after cudaDeviceReset on a device, do not call this there again.
+ * Every call reuses the same array: calls whose
  * kernels may overlap on the GPU (several streams or host threads) race on
  * it and must be serialised by the caller. */
 #define POA_NOALLOC_SCRATCH_BYTES (64u << 20)
@@ -227,6 +232,12 @@ int poa_align_noalloc(const poa_dev_window* w, const uint8_t* q_dev, int32_t qle
  * bytes, a multiple of 16 (row ring, staged records, query,
  * topsort workspace). Takes effect at the next run. */
 int poa_batch_config(poa_ctx* ctx, int32_t key, int64_t value);
+
+/* The measured int32 add+max rate of `device` (no counterpart in the
+ * reference): one timed launch of independent v = max(v + inc, floor)
+ * chains, 2 operations per step, `iters` steps per chain. It is the
+ * denominator of the DP's integer roofline. Allocates a small buffer. */
+int poa_int_peak(int device, int iters, double* ops_per_s, double* ms);
 
 /* Page-locked host memory (cudaMallocHost) for callers that want the
  * batch copies to run at full PCIe/NVLink-C2C speed; NULL on failure. */

@@ -142,6 +142,8 @@ def lib() -> ctypes.CDLL:
     L.poa_alloc_pinned.restype = ctypes.c_void_p
     L.poa_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
+    L.poa_int_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double)]
     _lib = L
     return L
 
@@ -437,6 +439,16 @@ def pinned_copy(a):
     h = PinnedArray(a.shape, a.dtype)
     h.array[...] = a
     return h, h.array
+
+
+def int_peak(device: int = 0, iters: int = 200000) -> Tuple[float, float]:
+    """Measured int32 add+max operations per second of `device` (the integer
+    roofline's denominator) and the timed launch's milliseconds."""
+    ops, ms = ctypes.c_double(), ctypes.c_double()
+    st = lib().poa_int_peak(device, iters, ctypes.byref(ops), ctypes.byref(ms))
+    if st != 0:
+        raise PoaError(st, "poa_int_peak")
+    return ops.value, ms.value
 
 
 def run(seqs: Sequence[bytes], params: Optional[Params] = None, headers=None, device: int = 0) -> bytes:

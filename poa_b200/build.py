@@ -22,7 +22,7 @@ CLI = os.path.join(PKG, "minipoa_b200")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
-CU_SRCS = ["gpu_engine.cu", "batch.cu", "noalloc.cu", "proposer.cu"]
+CU_SRCS = ["gpu_engine.cu", "batch.cu", "noalloc.cu", "proposer.cu", "intpeak.cu"]
 CPP_SRCS = ["graph.cpp", "driver.cpp", "seeding.cpp", "capi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
 

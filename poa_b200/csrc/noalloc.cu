@@ -21,6 +21,7 @@
 // caller.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <climits>
 #include <cstring>
 
@@ -35,19 +36,22 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[POA_NOALLOC_SCR
 // Device address of the scratch array, per device. In host code the symbol
 // g_noalloc_scratch is only a host-side stand-in, never a device address, so
 // it is resolved with cudaGetSymbolAddress once per device (with that device
-// current) on the first call there.
+// current) on the first call there. The cache is atomic: first calls from
+// several host threads may race to resolve it and store the same address.
+// The address belongs to the device's context: a process that calls
+// cudaDeviceReset on a device must not call poa_align_noalloc there again.
 constexpr int kMaxDevices = 64;
-static void* g_scratch_addr[kMaxDevices];
+static std::atomic<void*> g_scratch_addr[kMaxDevices];
 
 int scratch_for_current_device(void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return POA_CUDA;
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
+    void* p = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!p) {
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return POA_CUDA;
-        g_scratch_addr[dev] = p;
+        g_scratch_addr[dev].store(p, std::memory_order_release);
     }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return POA_OK;
 }
 
@@ -59,6 +63,8 @@ template <int NT>
 __global__ void __launch_bounds__(NT, 1) k_plain_noalloc(DpArgs a, const uint8_t* __restrict__ q, uint8_t* qs) {
     const int64_t qsb = qs_bytes(a.qlen);
     for (int64_t x = threadIdx.x; x < qsb; x += NT) qs[x] = (x >= 2 && x < (int64_t)a.qlen + 2) ? q[x - 2] : 4;
+    // score, move count and cells are only written on success: start them at 0
+    if (threadIdx.x < 3) a.out[1 + threadIdx.x] = 0;
     __syncthreads();
     if (a.v.n <= 0) {
         if (threadIdx.x == 0) a.out[0] = ST_BAD_ARG;
@@ -85,16 +91,24 @@ __global__ void __launch_bounds__(NT, 1) k_plain_noalloc(DpArgs a, const uint8_t
 namespace {
 
 // Worst-case scratch bytes of one window: every row at the full band width.
-int noalloc_need(int32_t n_rows, int32_t qlen, int32_t adaptive, int64_t* bytes) {
+// Every term is computed in int64 from values checked to be non-negative, so
+// no size can wrap; a window whose need exceeds `limit` stops the sum early.
+int noalloc_need(int32_t n_rows, int32_t qlen, int32_t adaptive, int64_t limit, int64_t* bytes) {
     if (n_rows <= 0 || qlen < 0 || !bytes) return POA_BAD_ARG;
-    const int64_t blocks = (int64_t)(qlen + 1) / pb::BLK + 1;  // widest possible row: the full band
-    int64_t need = (int64_t)pb::up256((size_t)pb::qs_bytes(qlen));
-    need += (int64_t)pb::up256(sizeof(pb::RowMeta) * (size_t)n_rows);
-    if (adaptive) need += (int64_t)pb::up256(4 * (size_t)pb::AB_NSTATE * n_rows);
-    need += (int64_t)pb::up256(4 * (size_t)(n_rows * blocks * 16 + 16));                 // row store
-    need += (int64_t)pb::up256((size_t)(n_rows * (blocks * pb::BLK * 4 + 16) + 16));     // records
+    const int64_t n = n_rows;
+    const int64_t blocks = ((int64_t)qlen + 1) / pb::BLK + 1;  // widest possible row: the full band
+    auto up = [](int64_t x) { return (x + 255) & ~(int64_t)255; };
+    int64_t need = up(pb::qs_bytes(qlen));
+    if (need > limit) { *bytes = need; return POA_OK; }
+    need += up((int64_t)sizeof(pb::RowMeta) * n);
+    if (adaptive) need += up(4 * (int64_t)pb::AB_NSTATE * n);
+    if (need > limit) { *bytes = need; return POA_OK; }
+    // blocks <= 2^28 and n < 2^31, so each product below stays under 2^63
+    need += up(4 * (n * blocks * 16 + 16));                 // row store
+    if (need > limit) { *bytes = need; return POA_OK; }
+    need += up(n * (blocks * pb::BLK * 4 + 16) + 16);       // records
     *bytes = need;
-    return POA_OK;
+    return need < 0 ? POA_BAD_ARG : POA_OK;
 }
 
 }  // namespace
@@ -108,10 +122,11 @@ extern "C" int poa_align_noalloc(const poa_dev_window* w, const uint8_t* q_dev, 
     if (!w->in_ptr || !w->in_row || !w->in_weight || !w->in_base || !w->base || !w->ind || !w->hq || !w->hq_loc ||
         !w->tq || !w->out_ptr || !w->out_row)
         return POA_BAD_ARG;
-    if (moves_cap < w->n_rows + qlen + 1) return POA_BAD_ARG;
+    if ((int64_t)moves_cap < (int64_t)w->n_rows + (int64_t)qlen + 1) return POA_BAD_ARG;
     const bool adaptive = p->band_f > 0 && ab_band;
     int64_t need = 0;
-    if (noalloc_need(w->n_rows, qlen, adaptive, &need) != POA_OK) return POA_BAD_ARG;
+    if (noalloc_need(w->n_rows, qlen, adaptive, (int64_t)POA_NOALLOC_SCRATCH_BYTES, &need) != POA_OK)
+        return POA_BAD_ARG;
     if (need > (int64_t)POA_NOALLOC_SCRATCH_BYTES) return POA_OOM;  // window too large for the fixed scratch
     void* base = nullptr;
     if (scratch_for_current_device(&base) != POA_OK) return POA_CUDA;

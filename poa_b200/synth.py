@@ -236,3 +236,34 @@ def write_fasta(path: str, seqs: Sequence[bytes], names: Sequence[str] = None) -
         for i, s in enumerate(seqs):
             nm = names[i] if names is not None else f"seq{i + 1}"
             fh.write(b">" + nm.encode() + b"\n" + s + b"\n")
+
+
+def write_pwin(path: str, ws: WindowSet, windows: Sequence[int] = None) -> None:
+    """Write windows to the flat binary window file the host-thread harnesses
+    read: b"PWIN", u32 n_windows, u32 n_reads, u32 win_off[n_windows + 1],
+    u32 read_len[n_reads], then the reads' ASCII bases back to back."""
+    if windows is not None:
+        ws = ws.subset(windows)
+    lens = ws.read_len.astype(np.uint32)
+    with open(path, "wb") as fh:
+        fh.write(b"PWIN")
+        fh.write(np.array([ws.n_windows, ws.n_reads], dtype=np.uint32).tobytes())
+        fh.write(ws.win_off.astype(np.uint32).tobytes())
+        fh.write(lens.tobytes())
+        if ws.n_reads:
+            a = int(ws.read_off[0])
+            b = int(ws.read_off[-1]) + int(ws.read_len[-1])
+            fh.write(ws.seq[a:b].tobytes())
+
+
+def read_cons_file(path: str) -> List[bytes]:
+    """Consensus strings of a window harness output (u32 length + bases each)."""
+    out: List[bytes] = []
+    with open(path, "rb") as fh:
+        data = fh.read()
+    p = 0
+    while p + 4 <= len(data):
+        n = int(np.frombuffer(data, dtype=np.uint32, count=1, offset=p)[0])
+        out.append(data[p + 4:p + 4 + n])
+        p += 4 + n
+    return out

@@ -5,6 +5,8 @@ reference's own sources into ``oracle/_ref/``):
 
     python tests/golden/make_golden.py              # small cases
     python tests/golden/make_golden.py --fullsize   # md5 of full-size runs
+    python tests/golden/make_golden.py --windows    # per-window manifests of the
+                                                    # full batched window sets
 
 For every case it writes ``<case>.fa`` (seeded synthetic input),
 ``<case>.out`` (the reference CLI's stdout, byte for byte: consensus, MSA or GFA) and, where the case
@@ -31,6 +33,7 @@ sys.path.insert(0, ROOT)
 from poa_b200 import synth  # noqa: E402
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "minipoa")
+POOL = os.path.join(ROOT, "oracle", "_ref", "ref_pool")
 HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
 
 
@@ -159,11 +162,49 @@ def fullsize():
         json.dump(out, fh, indent=1)
 
 
+# Full batched window sets (the benchmark's two workloads at full size): the
+# reference runs every window (oracle/_ref/ref_pool, one minipoa run per
+# window on all host threads) and the manifest keeps the first 16 hex digits
+# of each window's consensus md5, in window order.
+WINDOW_SETS = [
+    ("windows_polishing", "polishing_windows", dict(seed=4, n_windows=20000), []),
+    ("windows_learned_band", "learned_band_windows", dict(seed=5, n_windows=5000), ["-B"]),
+]
+
+
+def window_manifests(only=None):
+    import hashlib
+    import time
+    for name, gen, kw, opts in WINDOW_SETS:
+        if only and name not in only:
+            continue
+        ws = getattr(synth, gen)(**kw)
+        pw, co = os.path.join("/tmp", name + ".pwin"), os.path.join("/tmp", name + ".cons")
+        synth.write_pwin(pw, ws)
+        t0 = time.time()
+        res = subprocess.run([POOL] + opts + [pw, co], capture_output=True, text=True, check=True)
+        cons = synth.read_cons_file(co)
+        assert len(cons) == ws.n_windows, res.stdout
+        head = {"generator": gen, "kwargs": kw, "opts": opts, "windows": ws.n_windows,
+                "hash": "md5(consensus bases)[:16]", "reference_seconds": round(time.time() - t0, 1),
+                "pool": res.stdout.strip()}
+        with open(os.path.join(HERE, name + ".txt"), "w") as fh:
+            fh.write("# " + json.dumps(head) + "\n")
+            for c in cons:
+                fh.write(hashlib.md5(c).hexdigest()[:16] + "\n")
+        os.unlink(pw)
+        os.unlink(co)
+        print(name, head["reference_seconds"], "s")
+
+
 def main():
     if not (os.path.exists(REF_BIN) and os.path.exists(HARNESS)):
         sys.exit("build the reference first: make -C oracle ref")
     if "--fullsize" in sys.argv:
         fullsize()
+        return
+    if "--windows" in sys.argv:
+        window_manifests([a for a in sys.argv[1:] if not a.startswith("--")])
         return
     manifest = []
     for name, reads, opts, (base, base_names) in inc_cases():

@@ -59,3 +59,30 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(poa_b200, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(ImportError):
         poa_b200.lib()
+
+
+class _DevWindow(ctypes.Structure):
+    _fields_ = [("n_rows", ctypes.c_int32)] + [(f, ctypes.c_void_p) for f in (
+        "in_ptr", "in_row", "in_weight", "in_base", "base", "ind", "hq", "hq_loc", "tq", "out_ptr", "out_row")]
+
+
+@pytest.mark.parametrize("n_rows,qlen,moves_cap,want", [
+    (10, 2**31 - 1, 2**31 - 1, 3),          # moves capacity cannot hold n_rows + qlen + 1: POA_BAD_ARG
+    (10, 2**31 - 12, 2**31 - 1, 4),         # the query buffer alone exceeds the scratch: POA_OOM
+    (2**31 - 8, 1, 2**31 - 1, 4),           # row metadata alone exceeds the scratch: POA_OOM
+    (60000, 60000, 2**31 - 1, 4),           # rows x full band far beyond the scratch: POA_OOM
+    (10, -1, 100, 3),                       # negative query length: POA_BAD_ARG
+])
+def test_noalloc_size_checks_never_launch(lib, n_rows, qlen, moves_cap, want):
+    """poa_align_noalloc rejects impossible or oversized windows from their
+    sizes alone, before it touches the GPU (so this runs without one). The
+    pointers are never dereferenced on these paths."""
+    lib.poa_align_noalloc.argtypes = [ctypes.POINTER(_DevWindow), ctypes.c_void_p, ctypes.c_int32,
+                                      ctypes.POINTER(poa_b200._CParams), ctypes.c_int32, ctypes.c_void_p,
+                                      ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+    fake = ctypes.c_void_p(0x1000)
+    w = _DevWindow(n_rows, *([fake] * 11))
+    p = poa_b200._CParams()
+    lib.poa_params_init(ctypes.byref(p))
+    assert lib.poa_align_noalloc(ctypes.byref(w), fake, qlen, ctypes.byref(p), 0, fake, moves_cap, fake,
+                                 None) == want

@@ -160,42 +160,84 @@ def moves_to_res(a, n_rows, moves):
     return out
 
 
-def test_noalloc_matches_poa_align(oracle_bin):
-    torch = pytest.importorskip("torch")
-    if not torch.cuda.is_available():
-        pytest.skip("needs a CUDA device")
-    L = poa_b200.lib()
+def _bind(L):
     L.poa_align.argtypes = [ctypes.c_void_p, ctypes.POINTER(GraphView), ctypes.c_int32, ctypes.c_int32, PU8,
                             ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(Res), ctypes.c_int32, P32, P32]
     L.poa_align_noalloc.argtypes = [ctypes.POINTER(DevWindow), ctypes.c_void_p, ctypes.c_int32,
                                     ctypes.POINTER(poa_b200._CParams), ctypes.c_int32, ctypes.c_void_p,
                                     ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
-    ws = synth.windows(77, 2, (500, 600), (10, 12), 0.08)
-    calls = [(ws.window_reads(0), False), (ws.window_reads(1), True)]  # static band, then adaptive band
-    for reads, adaptive in calls:
-        a = build_graph(reads[:6])
-        query = np.frombuffer(bytes(reads[6]), dtype=np.uint8)
-        q_enc = np.array([{65: 0, 67: 1, 71: 2, 84: 3}.get(int(c), 4) for c in query], dtype=np.uint8)
-        params = poa_b200.Params(ab_band=adaptive)
-        cp = params._c()
-        # the existing entry point (host graph view)
-        with poa_b200.Context(params) as ctx:
-            gv = graph_view(a)
-            out = (Res * (a["base"].shape[0] + q_enc.shape[0] + 8))()
-            olen, score = ctypes.c_int32(), ctypes.c_int32()
-            st = L.poa_align(ctypes.c_void_p(ctx._h), ctypes.byref(gv), 0, 1, q_enc.ctypes.data_as(PU8),
-                             q_enc.shape[0], int(adaptive), out, len(out), ctypes.byref(olen), ctypes.byref(score))
-            assert st == 0
-            want = [(out[k].from_, out[k].base, out[k].aligned_id) for k in range(olen.value)]
-        # the allocation-free entry point on device-resident rows
-        n, rows = window_rows(a)
-        dev = {k: torch.from_numpy(v).cuda() for k, v in rows.items()}
-        dq = torch.from_numpy(q_enc.copy()).cuda()
-        cap = n + q_enc.shape[0] + 8
-        dmoves = torch.zeros(cap, dtype=torch.int32, device="cuda")
-        dres = torch.zeros(4, dtype=torch.int32, device="cuda")
-        w = DevWindow(n, *[dev[k].data_ptr() for k in ("in_ptr", "in_row", "in_weight", "in_base", "base", "ind",
-                                                       "hq", "hq_loc", "tq", "out_ptr", "out_row")])
+    return L
+
+
+def oracle_alignment(reads, query, adaptive):
+    """Score and path of the CPU restatement for `query` against the graph of
+    `reads` (the graph built as build_graph builds it, static band)."""
+    o = _oracle()
+    libc = ctypes.CDLL(None)
+    libc.free.argtypes = [ctypes.c_void_p]
+    p_graph = OParams(2, -4, -4, -2, 100, 40, 0, 0)
+    p_query = OParams(2, -4, -4, -2, 100, 40, int(adaptive), 0)
+    g = o.po_graph_new()
+    for i, r in enumerate(list(reads) + [query]):
+        last = i == len(reads)
+        q = np.frombuffer(bytes(r), dtype=np.uint8).copy()
+        path = ctypes.POINTER(ORes)()
+        plen, score = ctypes.c_int(), ctypes.c_int()
+        assert o.po_alignment(g, ctypes.byref(p_query if last else p_graph), q.ctypes.data_as(PU8), q.shape[0],
+                              ctypes.byref(path), ctypes.byref(plen), ctypes.byref(score)) == 0
+        res = [(path[k].from_, path[k].base, path[k].aligned_id) for k in range(plen.value)]
+        if not last:
+            o.po_add_path(g, i, path, plen.value, 1)
+            o.po_topsort(g, ctypes.byref(p_graph), 0)
+        libc.free(ctypes.cast(path, ctypes.c_void_p))
+    o.po_graph_free(g)
+    return score.value, res
+
+
+def noalloc_need(n_rows, qlen, adaptive):
+    """Worst-case scratch bytes of a window, as the entry point computes them."""
+    def up(x):
+        return (x + 255) // 256 * 256
+    m = qlen + 1
+    blocks = m // 8 + 1
+    need = up(((m // 8 + 3) * 8 + 15) // 16 * 16) + up(24 * n_rows)
+    if adaptive:
+        need += up(4 * 7 * n_rows)
+    return need + up(4 * (n_rows * blocks * 16 + 16)) + up(n_rows * (blocks * 8 * 4 + 16) + 16)
+
+
+SCRATCH = 64 << 20
+
+
+def encode(seq):
+    return np.array([{65: 0, 67: 1, 71: 2, 84: 3}.get(int(c), 4) for c in bytes(seq)], dtype=np.uint8)
+
+
+def align_both_ways(L, torch, reads, query, adaptive, q_pad=0):
+    """(score, path) of poa_align, and of two poa_align_noalloc calls in a row."""
+    a = build_graph(reads)
+    q_enc = encode(query)
+    params = poa_b200.Params(ab_band=adaptive)
+    cp = params._c()
+    with poa_b200.Context(params) as ctx:
+        gv = graph_view(a)
+        out = (Res * (a["base"].shape[0] + q_enc.shape[0] + 8))()
+        olen, score = ctypes.c_int32(), ctypes.c_int32()
+        st = L.poa_align(ctypes.c_void_p(ctx._h), ctypes.byref(gv), 0, 1, q_enc.ctypes.data_as(PU8),
+                         q_enc.shape[0], int(adaptive), out, len(out), ctypes.byref(olen), ctypes.byref(score))
+        assert st == 0
+        want = (score.value, [(out[k].from_, out[k].base, out[k].aligned_id) for k in range(olen.value)])
+    n, rows = window_rows(a)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in rows.items()}
+    dq = torch.zeros(q_enc.shape[0] + q_pad + 16, dtype=torch.uint8, device="cuda")
+    dq[:q_enc.shape[0]] = torch.from_numpy(q_enc.copy()).cuda()
+    cap = n + q_enc.shape[0] + q_pad + 8
+    w = DevWindow(n, *[dev[k].data_ptr() for k in ("in_ptr", "in_row", "in_weight", "in_base", "base", "ind",
+                                                   "hq", "hq_loc", "tq", "out_ptr", "out_row")])
+    got = []
+    for _ in range(2):
+        dmoves = torch.full((cap,), -1, dtype=torch.int32, device="cuda")
+        dres = torch.full((4,), -7, dtype=torch.int32, device="cuda")
         torch.cuda.synchronize()
         st = L.poa_align_noalloc(ctypes.byref(w), dq.data_ptr(), q_enc.shape[0], ctypes.byref(cp), int(adaptive),
                                  dmoves.data_ptr(), cap, dres.data_ptr(), None)
@@ -203,19 +245,67 @@ def test_noalloc_matches_poa_align(oracle_bin):
         torch.cuda.synchronize()
         res = dres.cpu().tolist()
         assert res[0] == 0, res
-        assert res[1] == score.value
-        got = moves_to_res(a, n, dmoves[:res[2]].cpu().numpy())
-        assert got == want
+        got.append((res[1], moves_to_res(a, n, dmoves[:res[2]].cpu().numpy())))
+    return n, want, got, (w, dq, cap, cp)
 
 
-def test_noalloc_rejects_oversized_window():
+def _cuda():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
-    L = poa_b200.lib()
-    L.poa_align_noalloc.argtypes = [ctypes.POINTER(DevWindow), ctypes.c_void_p, ctypes.c_int32,
-                                    ctypes.POINTER(poa_b200._CParams), ctypes.c_int32, ctypes.c_void_p,
-                                    ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
+    return torch
+
+
+def test_noalloc_matches_poa_align_and_oracle(oracle_bin):
+    torch = _cuda()
+    L = _bind(poa_b200.lib())
+    ws = synth.windows(77, 2, (500, 600), (10, 12), 0.08)
+    for w, adaptive in ((0, False), (1, True)):  # static band, then adaptive band
+        reads = ws.window_reads(w)
+        _, want, got, _ = align_both_ways(L, torch, reads[:6], reads[6], adaptive)
+        assert got[0] == want and got[1] == want
+        # and, independently of the CUDA entry points, the CPU restatement
+        assert oracle_alignment(reads[:6], reads[6], adaptive) == want
+
+
+def test_noalloc_window_at_the_scratch_limit(oracle_bin):
+    """A window whose worst case just fits the fixed scratch runs and matches;
+    a few query bases more and the call is refused before any launch."""
+    torch = _cuda()
+    L = _bind(poa_b200.lib())
+    ws = synth.windows(78, 1, (600, 600), (7, 7), 0.08)
+    reads = ws.window_reads(0)
+    a = build_graph(reads[:6])
+    n = int(a["rank"][1]) - int(a["rank"][0]) + 1
+    qlen = 1
+    while noalloc_need(n, qlen + 1, False) <= SCRATCH:
+        qlen += 1
+    assert noalloc_need(n, qlen, False) > SCRATCH - (1 << 20)  # within 1 MiB of the limit
+    # the last read with a random insertion in its middle, up to qlen bases
+    r = reads[6]
+    rng = np.random.default_rng(79)
+    ins = synth.to_ascii(synth.random_root(rng, qlen - len(r)))
+    query = r[:len(r) // 2] + ins + r[len(r) // 2:]
+    assert len(query) == qlen
+    n2, want, got, (w, dq, cap, cp) = align_both_ways(L, torch, reads[:6], query, False, q_pad=64)
+    assert n2 == n
+    assert got[0] == want and got[1] == want
+    assert oracle_alignment(reads[:6], query, False) == want
+    # 8 more bases: one more block per row no longer fits; refused (POA_OOM), nothing launched
+    assert noalloc_need(n, qlen + 8, False) > SCRATCH
+    dres = torch.full((4,), -7, dtype=torch.int32, device="cuda")
+    dmoves = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    st = L.poa_align_noalloc(ctypes.byref(w), dq.data_ptr(), qlen + 8, ctypes.byref(cp), 0, dmoves.data_ptr(),
+                             cap, dres.data_ptr(), None)
+    assert st == 4
+    torch.cuda.synchronize()
+    assert dres.cpu().tolist() == [-7, -7, -7, -7]
+
+
+def test_noalloc_rejects_oversized_window():
+    torch = _cuda()
+    L = _bind(poa_b200.lib())
     # 20,000 rows x a 10 kb query needs far more than the fixed scratch: POA_OOM, nothing launched
     dummy = torch.zeros(16, dtype=torch.int32, device="cuda")
     p = dummy.data_ptr()

@@ -22,9 +22,11 @@ e2e    windows/s through the public C ABI (poa_batch_consensus) with the
 plain_kernel  windows/s of the plain single-alignment kernel path (poa_run:
        one CTA per poa() call, graph fused on the host) on a sample of the
        same windows, and the batched engine's speed-up over it.
-Multi-GPU: every rank runs its own windows (weak scaling, no collective on
-the data path; torch.distributed only for the barrier and the max over ranks
-of the time).
+Multi-GPU: one set of N x 5,000 windows, split over the ranks by cost
+(poa_batch_partition; weak scaling: the work per GPU stays fixed); no
+collective on the data path: torch.distributed gives the barrier, the max
+over ranks of the time, and the gather of the consensus strings (in window
+order) after the timed region for the parity check.
 ``--impl reference`` times the reference's own CPU build (oracle/_ref/minipoa,
 compiled from the reference sources) on a bounded sample of the same
 windows with every host core, one process per window.
@@ -49,6 +51,7 @@ sys.path.insert(0, ROOT)
 METRIC = "windows/s & GCUPS on 1 B200: learned-band+batched vs plain kernel, bit-exact"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "minipoa")
 PORT_BIN = os.path.join(ROOT, "oracle", "build", "poa_oracle")
+POOL_BIN = os.path.join(ROOT, "oracle", "_ref", "ref_pool")
 # algorithmic work per DP cell: 1 byte of traceback record written
 # (cell = one computed band cell, (Be-Bs-1)*8 per row)
 BYTES_PER_CELL = 1.0
@@ -58,13 +61,15 @@ OPS_PER_CELL, OPS_PER_EDGE_CELL = 5, 7
 WORKLOADS = {
     "learned_band": {
         "gen": "learned_band_windows", "seed": 5, "windows": 5000, "opts": ["-B"], "proposer": True,
-        "steps": 1, "ref_windows_per_core": 1,
+        "manifest": "windows_learned_band",
+        "steps": 1, "ref_windows_per_core": 2, "ref_sample_per_core": 8,
         "desc": "learned_band_windows: 5000 windows, template 2000 bp, 20-100 reads, 15% error (4:3:3), "
                 "1% chimeric reads; adaptive band -B; consensus",
         "mode": "consensus, adaptive band (-B) b=100 f=40, learned band proposer sizes the slots"},
     "polishing": {
         "gen": "polishing_windows", "seed": 4, "windows": 20000, "opts": [], "proposer": False,
-        "steps": 5, "ref_windows_per_core": 40,
+        "manifest": "windows_polishing",
+        "steps": 5, "ref_windows_per_core": 40, "ref_sample_per_core": 400,
         "desc": "polishing_windows: 20000 windows, template 500+-100 bp, 4-64 reads, 8% error (4:3:3), consensus",
         "mode": "consensus, static band b=100 f=40"},
 }
@@ -74,14 +79,30 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
-def shard_seed(rank: int, base: int = 5) -> int:
-    """Seed of rank r's windows: every rank runs its own windows (weak scaling)."""
-    return base + 1000 * rank
+def rank_windows(ws, world: int, rank: int):
+    """This rank's share of one window set: the cost-balanced split of
+    poa_batch_partition (longest processing time first), in input order."""
+    import numpy as np
+    if world == 1:
+        return np.arange(ws.n_windows)
+    import poa_b200
+    part, _ = poa_b200.partition(ws, world)
+    return np.nonzero(part == rank)[0]
 
 
-def whole_job_rate(world: int, units_per_rank: int, steps: int, t_max: float) -> float:
-    """Units per second over all ranks, timed by the slowest rank."""
-    return world * units_per_rank * steps / t_max
+def gather_in_order(D, idx, items, n_total):
+    """Per-window results of every rank, back in the window set's order."""
+    pairs = D.gather_objects(list(zip([int(i) for i in idx], items)))
+    out = [None] * n_total
+    for part in pairs:
+        for i, v in part:
+            out[i] = v
+    return out
+
+
+def whole_job_rate(total_units: int, steps: int, t_max: float) -> float:
+    """Units per second of the whole job (all ranks' units), timed by the slowest rank."""
+    return total_units * steps / t_max
 
 
 def dist_env():
@@ -131,6 +152,14 @@ class Dist:
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t)
         return float(t.item())
+
+    def gather_objects(self, obj):
+        """Every rank's `obj`, in rank order (all ranks take part)."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world
+        self.pg.all_gather_object(out, obj)
+        return out
 
     def close(self):
         if self.pg:
@@ -246,24 +275,53 @@ def run_cpu_windows(binary, paths, cores, opts=()):
         return list(ex.map(one, paths))
 
 
-def cpu_sample(ws, seconds, cores, binary, opts=(), chunk_per_core=4):
-    """Windows/s of the CPU binary over windows 0, 1, ... of ws: chunks of
-    `chunk_per_core` windows per core until about `seconds` of wall time."""
-    outs = []
-    n = 0
-    with tempfile.TemporaryDirectory() as d:
-        t0 = time.perf_counter()
-        while n < ws.n_windows and time.perf_counter() - t0 < seconds:
-            idx = range(n, min(ws.n_windows, n + chunk_per_core * cores))
-            outs.extend(run_cpu_windows(binary, write_windows(ws, idx, d), cores, opts))
-            n = idx.stop
-        dt = time.perf_counter() - t0
-    return n / dt, n, dt, outs
-
-
-def make_windows(wl, rank, n, reads_per_window=0):
+def run_pool(pwin, opts, cores, first, n, seconds=None):
+    """One oracle/_ref/ref_pool run: the reference library (one minipoa run
+    per window) on `cores` host threads pulling windows first .. first+n-1
+    continuously. Returns (windows done, wall s, summed per-window thread s,
+    consensus of the leading done windows)."""
     from poa_b200 import synth
-    ws = getattr(synth, wl["gen"])(seed=shard_seed(rank, wl["seed"]), n_windows=n)
+    out = pwin + ".cons"
+    cmd = [POOL_BIN] + (["-B"] if "-B" in opts else []) + ["-t", str(cores), "-f", str(first), "-n", str(n)]
+    if seconds:
+        cmd += ["-s", str(seconds)]
+    res = subprocess.run(cmd + [pwin, out], capture_output=True, text=True, check=True)
+    f = res.stdout.split()
+    kv = dict(zip(f[0::2], f[1::2]))
+    cons = synth.read_cons_file(out)
+    os.unlink(out)
+    return int(kv["windows"]), float(kv["seconds"]), float(kv["busy"]), cons
+
+
+def cpu_sample(ws, seconds, cores, opts, per_core):
+    """The reference on this host's cores over the first windows of ws, for
+    about `seconds`: (sustained windows/s = done / (thread time / threads),
+    windows done, wall s, their consensus). Without the compiled reference
+    the restatement runs instead, one process per window."""
+    from poa_b200 import synth
+    n = min(ws.n_windows, per_core * cores)
+    if os.path.exists(POOL_BIN):
+        with tempfile.TemporaryDirectory() as d:
+            pw = os.path.join(d, "w.pwin")
+            synth.write_pwin(pw, ws, range(n))
+            done, wall, busy, cons = run_pool(pw, opts, cores, 0, n, seconds)
+        return "reference", done * cores / busy, done, wall, cons
+    outs = []
+    k = 0
+    with tempfile.TemporaryDirectory() as d:
+        paths = write_windows(ws, range(n), d)
+        t0 = time.perf_counter()
+        while k < n and time.perf_counter() - t0 < seconds:
+            idx = range(k, min(n, k + cores))
+            outs.extend(o.split(b"\n")[1] for o in run_cpu_windows(PORT_BIN, [paths[w] for w in idx], cores, opts))
+            k = idx.stop
+        dt = time.perf_counter() - t0
+    return "port", k / dt, k, dt, outs
+
+
+def make_windows(wl, n, reads_per_window=0):
+    from poa_b200 import synth
+    ws = getattr(synth, wl["gen"])(seed=wl["seed"], n_windows=n)
     if reads_per_window > 0:
         # small profiling captures: the first reads of every window
         reads, offs = [], [0]
@@ -275,6 +333,24 @@ def make_windows(wl, rank, n, reads_per_window=0):
     return ws
 
 
+def manifest_check(wl, cons):
+    """Windows whose consensus matches the reference's per-window manifest
+    (tests/golden/<manifest>.txt, md5[:16] of each window's consensus, made
+    by tests/golden/make_golden.py --windows from the reference binary)."""
+    import hashlib
+    p = os.path.join(ROOT, "tests", "golden", wl["manifest"] + ".txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        head = json.loads(fh.readline()[2:])
+        want = [ln.strip() for ln in fh]
+    if head["kwargs"]["seed"] != wl["seed"]:
+        return None
+    n = min(len(want), len(cons))
+    same = sum(1 for w in range(n) if hashlib.md5(cons[w]).hexdigest()[:16] == want[w])
+    return {"windows": n, "identical_consensus": same, "manifest": os.path.relpath(p, ROOT)}
+
+
 # --------------------------------------------------------------------- arms
 def ours(args, world, rank, local, D):
     import poa_b200
@@ -282,8 +358,12 @@ def ours(args, world, rank, local, D):
     wl = WORKLOADS[args.workload]
     nwin = args.windows or wl["windows"]
     t0 = time.perf_counter()
-    ws = make_windows(wl, rank, nwin, args.reads_per_window)
-    log(f"[rank {rank}] generated {ws.n_windows} windows / {ws.n_reads} reads in {time.perf_counter() - t0:.1f}s")
+    # one window set of nwin windows per GPU, split over the ranks by cost
+    full = make_windows(wl, nwin * world, args.reads_per_window)
+    mine = rank_windows(full, world, rank)
+    ws = full if world == 1 else full.subset(mine)
+    log(f"[rank {rank}] generated {full.n_windows} windows, this rank runs {ws.n_windows} / {ws.n_reads} reads "
+        f"in {time.perf_counter() - t0:.1f}s")
     try:
         import torch
         torch.cuda.set_device(local)
@@ -334,6 +414,9 @@ def ours(args, world, rank, local, D):
     cells = st["cells"]
     failed = int(D.sum(st["failed"]))
     cons, status = ctx.batch_download()
+    # every window of the whole set against the reference's per-window manifest
+    all_cons = cons if world == 1 else gather_in_order(D, mine, cons, full.n_windows)
+    parity_full = manifest_check(wl, all_cons) if (rank == 0 and not args.reads_per_window) else None
     # proposer kernels per step: features, 3 im2col + 5 GEMM + pool + de-standardise
     # per 4096-read chunk, conversion, plan
     if prop is not None:
@@ -360,7 +443,7 @@ def ours(args, world, rank, local, D):
         D.barrier()
         t_e2e = D.max(time.perf_counter() - t0)
         st2 = ctx.batch_stats()
-        e2e = {"value": whole_job_rate(world, ws.n_windows, args.steps, t_e2e), "unit": "windows/s",
+        e2e = {"value": whole_job_rate(full.n_windows, args.steps, t_e2e), "unit": "windows/s",
                "h2d_bytes_per_step": int(st2["h2d_bytes"]), "d2h_bytes_per_step": int(st2["d2h_bytes"]),
                "ms_per_step": 1e3 * t_e2e / args.steps, "api": "poa_batch_consensus", "warmup": e2e_warm,
                "note": "host wall clock around upload + plan + kernel + download"
@@ -369,7 +452,8 @@ def ours(args, world, rank, local, D):
         for h in holders:
             h.close()
 
-    value = whole_job_rate(world, ws.n_windows, args.steps, t_dev)
+    value = whole_job_rate(full.n_windows, args.steps, t_dev)
+    cells_all = D.sum(cells)
     kernel_s = D.max(sum(kern_ms) / 1e3) / args.steps
     peaks = load_peaks()
     achieved = cells * BYTES_PER_CELL / kernel_s / 1e9
@@ -399,12 +483,14 @@ def ours(args, world, rank, local, D):
                    "windows_per_rank": ws.n_windows, "reads_per_rank": ws.n_reads,
                    "bases_per_rank": int(ws.seq.shape[0]), "mode": wl["mode"] if prop else
                    wl["mode"].replace(", learned band proposer sizes the slots", ""),
-                   "parallelism": f"windows sharded over {world} GPU(s)",
+                   "parallelism": f"one set of {full.n_windows} windows split over {world} GPU(s) by cost "
+                                  "(poa_batch_partition)",
                    "l2": "inputs (%.0f MB) and slots (%.1f GB) larger than L2 (126 MB)"
                          % (ws.seq.shape[0] / 1e6, st["slots"] * st["slot_bytes"] / 1e9)},
-        "gcups": world * cells * args.steps / t_dev / 1e9,
+        "gcups": cells_all * args.steps / t_dev / 1e9,
         "cells_per_step": cells, "failed_windows": failed,
         "gpu_launches": launches, "retried_windows": st["retried"], "e2e": e2e, "roofline": roofline, "clocks": clocks,
+        "parity_full": parity_full,
         "slots": st["slots"], "slot_bytes": st["slot_bytes"], "launch_shape": shape,
         "phase_share": {k: v / max(1, sum(st["phase_cycles"].values())) for k, v in st["phase_cycles"].items()},
         "phase_mcycles_per_window": {k: v / 1e6 / ws.n_windows for k, v in st["phase_cycles"].items()},
@@ -428,55 +514,78 @@ def ours(args, world, rank, local, D):
                                 "path": "poa_run: one CTA per poa() call (k_plain_static for the static band, k_plain for -B), graph fused on the host",
                                 "speedup": value / (n / dt)}
     if rank == 0 and world == 1 and not args.no_cpu:
-        binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
-        kind = "reference" if binary == REF_BIN else "port"
         cores = len(os.sched_getaffinity(0))
-        v, n, dt, outs = cpu_sample(ws, args.cpu_seconds, cores, binary, wl["opts"],
-                                    chunk_per_core=1 if wl["proposer"] else 4)
-        same = sum(1 for w in range(n) if outs[w] == b">consensus sequence\n" + cons[w] + b"\n")
+        kind, v, n, dt, outs = cpu_sample(ws, args.cpu_seconds, cores, wl["opts"], wl["ref_sample_per_core"])
+        same = sum(1 for w in range(n) if outs[w] == cons[w])
         line["cpu_baseline"] = {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
-                                "sample": f"first {n} of the {ws.n_windows} windows, one process per window "
-                                          f"({' '.join(wl['opts']) or 'default options'}), {dt:.1f}s wall"}
+                                "sample": f"first {n} of the {ws.n_windows} windows "
+                                          f"({' '.join(wl['opts']) or 'default options'}), "
+                                          + ("oracle/_ref/ref_pool: the reference library, one minipoa run per "
+                                             f"window, {cores} threads pulling windows; windows / (thread time / "
+                                             f"threads); {dt:.1f}s wall, {n / dt:.3f} windows/s by wall clock"
+                                             if kind == "reference" else
+                                             f"the restatement, one process per window, {dt:.1f}s wall")}
         line["parity_sample"] = {"windows": n, "identical_consensus": same}
     ctx.close()
     return line
 
 
 def reference(args, world, rank, local, D):
+    """The reference's own CPU build on this host's cores (rank 0 only): each
+    step runs the next windows of the same seeded set through
+    oracle/_ref/ref_pool (the reference library, one minipoa run per window,
+    every host thread pulling windows). The rate counts every thread busy:
+    windows / (summed per-window thread time / threads); the wall-clock rate
+    is reported beside it."""
     if rank != 0:
         return None
+    from poa_b200 import synth
     wl = WORKLOADS[args.workload]
-    binary = REF_BIN if os.path.exists(REF_BIN) else PORT_BIN
-    kind = "reference" if binary == REF_BIN else "port"
     cores = len(os.sched_getaffinity(0))
     per_step = min(args.windows or wl["windows"], wl["ref_windows_per_core"] * cores)
     # every step (warm-up ones too) takes the next windows of the seeded set, so the
     # timed steps see windows of every size rather than the same few again
     total = min(args.windows or wl["windows"], per_step * (args.warmup + args.steps))
-    ws = make_windows(wl, 0, total)
-    chunk = lambda k: range((k * per_step) % total, min((k * per_step) % total + per_step, total))
+    ws = make_windows(wl, total)
+    first = lambda k: (k * per_step) % total
+    done = 0
+    busy_s = wall_s = 0.0
     with tempfile.TemporaryDirectory() as d:
-        paths = write_windows(ws, range(total), d)
-        for k in range(args.warmup):
-            run_cpu_windows(binary, [paths[w] for w in chunk(k)], cores, wl["opts"])
-        t0 = time.perf_counter()
-        done = 0
-        for k in range(args.warmup, args.warmup + args.steps):
-            idx = chunk(k)
-            run_cpu_windows(binary, [paths[w] for w in idx], cores, wl["opts"])
-            done += len(idx)
-        dt = time.perf_counter() - t0
-    per_step = done / max(args.steps, 1)
-    v = done / dt
+        pw = os.path.join(d, "w.pwin")
+        synth.write_pwin(pw, ws)
+        if os.path.exists(POOL_BIN):
+            kind = "reference"
+            for k in range(args.warmup):
+                run_pool(pw, wl["opts"], cores, first(k), per_step)
+            for k in range(args.warmup, args.warmup + args.steps):
+                n, wall, busy, _ = run_pool(pw, wl["opts"], cores, first(k), per_step)
+                done += n
+                busy_s += busy / cores
+                wall_s += wall
+        else:
+            kind = "port"
+            paths = write_windows(ws, range(total), d)
+            t0 = time.perf_counter()
+            for k in range(args.warmup, args.warmup + args.steps):
+                idx = range(first(k), min(first(k) + per_step, total))
+                run_cpu_windows(PORT_BIN, [paths[w] for w in idx], cores, wl["opts"])
+                done += len(idx)
+            busy_s = wall_s = time.perf_counter() - t0
+    v = done / busy_s
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "windows/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * busy_s / args.steps,
+            "wall_ms_per_step": 1e3 * wall_s / args.steps, "wall_value": done / wall_s,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded; no dataset)",
-            "config": {"workload": wl["desc"], "windows_per_step": per_step, "mode": wl["mode"],
-                       "sample": f"{done} windows in {args.steps} steps, the next {per_step:.0f} of the seeded set each"},
+            "config": {"workload": wl["desc"], "windows_per_step": done / max(args.steps, 1), "mode": wl["mode"],
+                       "sample": f"{done} windows in {args.steps} steps, the next {per_step} of the seeded set each"},
             "cpu_baseline": {"value": v, "unit": "windows/s", "cores": cores, "kind": kind,
-                             "sample": f"{per_step} windows per step, one {kind} process per window "
-                                       f"({' '.join(wl['opts']) or 'default options'}), {cores} concurrent"},
+                             "sample": f"{per_step} windows per step "
+                                       f"({' '.join(wl['opts']) or 'default options'}); "
+                                       + ("oracle/_ref/ref_pool: the reference library, one minipoa run per window, "
+                                          f"{cores} threads pulling windows; rate = windows / (thread time / threads), "
+                                          f"{done / wall_s:.3f} windows/s by wall clock"
+                                          if kind == "reference" else "the restatement, one process per window")},
             "e2e": {"value": v, "unit": "windows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

@@ -250,6 +250,22 @@ void poa_free_pinned(void* ptr);
 int poa_stats(const poa_ctx* ctx, int64_t* out6);
 int poa_set_timing(poa_ctx* ctx, int on);
 
+/* One window set over several GPUs (no counterpart in the reference, which
+ * runs one graph per process; configurations with independent windows shard
+ * across devices with no exchange between them). poa_batch_partition splits
+ * windows by estimated cost (bases x (reads + 1)) with the longest-
+ * processing-time rule: part[w] in [0, n_parts), part_cost[g] (may be NULL)
+ * the summed cost of part g. poa_batch_consensus_multi runs part g on
+ * ctxs[g] (one context per device, each on its own host thread) and writes
+ * the same outputs as poa_batch_consensus, in input order. Every device gets
+ * the whole seq buffer; read_off may point anywhere in it. */
+int poa_batch_partition(const int32_t* read_len, const int32_t* win_off, int32_t n_windows, int32_t n_parts,
+                        int32_t* part, int64_t* part_cost);
+int poa_batch_consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const uint8_t* seq, int64_t seq_bytes,
+                              const int64_t* read_off, const int32_t* read_len, int32_t n_reads,
+                              const int32_t* win_off, int32_t n_windows, char* cons, int64_t cons_cap,
+                              int64_t* cons_off, int32_t* status);
+
 /* ---- learned band proposer (no counterpart in the reference) -----------
  *
  * minipoa allocates each alignment's DP matrices when it runs it

@@ -13,14 +13,18 @@
 // batches); each thread owns its aligned_buff_t arena, as src/main.cpp:109
 // gives one per thread.
 //
-// Usage: ref_pool [-B] [-t threads] [-n max_windows] [-s seconds] in.pwin out.cons
+// Usage: ref_pool [-B] [-t threads] [-f first] [-n max_windows] [-s seconds] in.pwin out.cons
 //   in.pwin   "PWIN" u32 n_windows, u32 n_reads, u32 win_off[n_windows+1],
 //             u32 read_len[n_reads], then the reads' ASCII bases back to back
 //   out.cons  per processed window in input order: u32 length, then the bases
-//   -n        process only the first max_windows windows
+//   -f / -n   process windows first .. first + max_windows - 1 only
 //   -s        stop handing out windows after `seconds` (timing samples)
-// Prints one line to stdout: "windows <n> seconds <wall> threads <t>", the
-// wall time of the pool (file I/O excluded).
+// Prints one line to stdout: "windows <n> seconds <wall> threads <t> prefix
+// <p> busy <b>": windows done, the wall time of the pool (file I/O
+// excluded), the length of the leading run of done windows written to
+// out.cons, and the summed per-window thread time (windows * threads / busy
+// is the pool's rate with every thread kept busy, free of the tail where
+// the last windows finish on fewer threads).
 #include <atomic>
 #include <chrono>
 #include <cstdint>
@@ -38,7 +42,7 @@ static bool read_all(FILE* f, void* p, size_t n) { return std::fread(p, 1, n, f)
 int main(int argc, char** argv) {
     bool ab = false;
     int threads = (int)std::thread::hardware_concurrency();
-    long max_win = -1;
+    long max_win = -1, first = 0;
     double seconds = -1.0;
     std::vector<std::string> pos;
     for (int a = 1; a < argc; a++) {
@@ -46,6 +50,7 @@ int main(int argc, char** argv) {
         if (o == "-B") ab = true;
         else if (o == "-t" && a + 1 < argc) threads = std::atoi(argv[++a]);
         else if (o == "-n" && a + 1 < argc) max_win = std::atol(argv[++a]);
+        else if (o == "-f" && a + 1 < argc) first = std::atol(argv[++a]);
         else if (o == "-s" && a + 1 < argc) seconds = std::atof(argv[++a]);
         else pos.push_back(o);
     }
@@ -71,7 +76,9 @@ int main(int argc, char** argv) {
     std::string bases(roff[nr], '\0');
     if (!read_all(f, &bases[0], bases.size())) { std::fprintf(stderr, "truncated bases\n"); return 2; }
     std::fclose(f);
-    const uint32_t todo = max_win >= 0 && (uint64_t)max_win < nw ? (uint32_t)max_win : nw;
+    if (first < 0 || (uint64_t)first > nw) { std::fprintf(stderr, "bad -f\n"); return 2; }
+    const uint32_t avail = nw - (uint32_t)first;
+    const uint32_t todo = max_win >= 0 && (uint64_t)max_win < avail ? (uint32_t)max_win : avail;
 
     // the CLI defaults of src/main.cpp:16-33 (-M 2 -X -4 -O -4 -E -2 -b 100 -f 40)
     para_t* para = new para_t();
@@ -84,14 +91,17 @@ int main(int argc, char** argv) {
     std::vector<std::string> cons(todo);
     std::vector<char> done(todo, 0);
     std::atomic<uint32_t> next(0);
+    std::vector<double> busy(threads, 0.0);
     const auto t0 = std::chrono::steady_clock::now();
     auto elapsed = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
-    auto worker = [&]() {
+    auto worker = [&](int tid) {
         aligned_buff_t mpool;
         while (true) {
             if (seconds >= 0.0 && elapsed() >= seconds) break;
-            const uint32_t w = next.fetch_add(1);
-            if (w >= todo) break;
+            const uint32_t k = next.fetch_add(1);
+            if (k >= todo) break;
+            const double tw0 = elapsed();
+            const uint32_t w = k + (uint32_t)first;
             std::vector<seq_t> seqs(win_off[w + 1] - win_off[w]);
             for (uint32_t r = win_off[w]; r < win_off[w + 1]; r++) {
                 seq_t& s = seqs[r - win_off[w]];
@@ -109,14 +119,15 @@ int main(int argc, char** argv) {
                 DAG->topsort(para, i + 1 == seqs.size());
             }
             DAG->build_consensus();
-            cons[w] = DAG->cons;
-            done[w] = 1;
+            cons[k] = DAG->cons;
+            done[k] = 1;
+            busy[tid] += elapsed() - tw0;
             delete mm;
             delete DAG;
         }
     };
     std::vector<std::thread> pool;
-    for (int t = 0; t < threads; t++) pool.emplace_back(worker);
+    for (int t = 0; t < threads; t++) pool.emplace_back(worker, t);
     for (auto& t : pool) t.join();
     const double wall = elapsed();
 
@@ -132,6 +143,8 @@ int main(int argc, char** argv) {
     std::fclose(o);
     uint32_t total = 0;
     for (uint32_t w = 0; w < todo; w++) total += done[w];
-    std::printf("windows %u seconds %.6f threads %d prefix %u\n", total, wall, threads, ndone);
+    double busy_total = 0.0;
+    for (double b : busy) busy_total += b;
+    std::printf("windows %u seconds %.6f threads %d prefix %u busy %.6f\n", total, wall, threads, ndone, busy_total);
     return 0;
 }

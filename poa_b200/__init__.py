@@ -144,6 +144,10 @@ def lib() -> ctypes.CDLL:
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
     L.poa_int_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(ctypes.c_double)]
+    L.poa_batch_partition.argtypes = [_i32p, _i32p, ctypes.c_int32, ctypes.c_int32, _i32p, _i64p]
+    L.poa_batch_consensus_multi.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, _u8p, ctypes.c_int64,
+                                            _i64p, _i32p, ctypes.c_int32, _i32p, ctypes.c_int32, ctypes.c_void_p,
+                                            ctypes.c_int64, _i64p, _i32p]
     _lib = L
     return L
 
@@ -439,6 +443,47 @@ def pinned_copy(a):
     h = PinnedArray(a.shape, a.dtype)
     h.array[...] = a
     return h, h.array
+
+
+def partition(ws, n_parts: int):
+    """Split a window set over n_parts devices by estimated cost
+    (poa_batch_partition: longest processing time first). Returns (part of
+    each window as an int32 array, summed cost of each part)."""
+    import numpy as np
+    rlen = np.ascontiguousarray(ws.read_len, dtype=np.int32)
+    woff = np.ascontiguousarray(ws.win_off, dtype=np.int32)
+    nwin = int(woff.shape[0] - 1)
+    part = np.zeros(max(nwin, 1), dtype=np.int32)
+    cost = np.zeros(n_parts, dtype=np.int64)
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    st = lib().poa_batch_partition(rlen.ctypes.data_as(i32p), woff.ctypes.data_as(i32p), nwin, n_parts,
+                                   part.ctypes.data_as(i32p), cost.ctypes.data_as(i64p))
+    if st != 0:
+        raise PoaError(st, "poa_batch_partition")
+    return part[:nwin], cost
+
+
+def batch_consensus_multi(contexts: Sequence["Context"], ws):
+    """One window set over several devices (poa_batch_consensus_multi: a
+    cost-balanced split, one context per device on its own host thread, the
+    consensus gathered in input order). Returns (consensus bytes, status) per
+    window, as Context.batch_consensus does."""
+    import numpy as np
+    seq, roff, rlen, woff = Context._win_arrays(ws)
+    nwin = int(woff.shape[0] - 1)
+    cap = int(2 * (int(rlen.max()) if rlen.shape[0] else 0) + 64) * max(nwin, 1)
+    cons = ctypes.create_string_buffer(max(cap, 1))
+    off = np.zeros(nwin + 1, dtype=np.int64)
+    st = np.zeros(max(nwin, 1), dtype=np.int32)
+    hs = (ctypes.c_void_p * len(contexts))(*[c._h for c in contexts])
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    rc = lib().poa_batch_consensus_multi(hs, len(contexts), seq.ctypes.data, seq.shape[0], roff.ctypes.data_as(i64p),
+                                         rlen.ctypes.data_as(i32p), rlen.shape[0], woff.ctypes.data_as(i32p), nwin,
+                                         cons, cap, off.ctypes.data_as(i64p), st.ctypes.data_as(i32p))
+    if rc != 0:
+        raise PoaError(rc, "poa_batch_consensus_multi")
+    raw = cons.raw
+    return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
 
 
 def int_peak(device: int = 0, iters: int = 200000) -> Tuple[float, float]:

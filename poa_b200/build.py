@@ -23,7 +23,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SRCS = ["gpu_engine.cu", "batch.cu", "noalloc.cu", "proposer.cu", "intpeak.cu"]
-CPP_SRCS = ["graph.cpp", "driver.cpp", "seeding.cpp", "capi.cpp"]
+CPP_SRCS = ["graph.cpp", "driver.cpp", "seeding.cpp", "capi.cpp", "multi.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

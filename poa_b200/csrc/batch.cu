@@ -1085,6 +1085,283 @@ __device__ __forceinline__ void fill_row(const DpArgs& a, const RowDesc& cur, co
     }
 }
 
+// One row of the adaptive / full-band warp fill (dp_fill_warp_dyn): the chunk
+// loop of fill_row, with the predecessors' records `er` (backtrack priority
+// order, bands and row-store locations patched in) read once per chunk, and
+// the record choices of multi-predecessor rows kept in one pass
+// (dp_core.h track_d / track_m): per cell the running maximum of each kind
+// of term plus a 4-bit first position per choice, folded into one 16-bit
+// word (z) as soon as the predecessors are read:
+//   z bits 0..3 D choice (dopen, else dext; 15 none), bit 4 W_DEXT,
+//          8..11 m4, 12..15 m1 (15 none; gated by M == Mpre at the record).
+// Register roles by row kind: with one predecessor Mpre / Dv are the
+// diagonal / vertical maxima and pa / pb copies of its M / D block (for the
+// 1-byte records); with several, Mpre is the diagonal maximum, Dv the
+// maximum of M_p + o1, pb of D_p + e1 and pa of the matching diagonal terms
+// until the pass ends, when Dv becomes the vertical maximum.
+// Rows with more than TRACK_MAX_D predecessors, and blocks where the fill's
+// block-granular masks differ from the backtrack's per-cell test, take the
+// second pass over the predecessors (as fill_row does).
+template <bool ARGMAX>
+__device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur, const int4* __restrict__ er,
+                                             const uint8_t* __restrict__ qsm, int i, int lane, int32_t& bestM,
+                                             int& bestJ) {
+    const Scoring sc = a.sc;
+    const int32_t K = add32(add32(NEG_INF, sc.e1), -sc.o1);
+    const int Bs = cur.bsbe & 0xffff, Be = cur.bsbe >> 16, bn = Be - Bs - 1;
+    const int d = cur.d;
+    const bool multi = d >= 2;
+    int32_t* dst = a.rs + cur.st;
+    const int nch = (bn + 31) >> 5;
+    int32_t carryP = K, carryM = NEG_INF, carryI = NEG_INF;
+    for (int c = 0; c < nch; c++) {
+        const int b = c * 32 + lane;
+        const bool act = b < bn;
+        const int B = Bs + b;
+        const int j0 = b * BLK;
+        int32_t Mpre[BLK], Dv[BLK], H0[BLK], M[BLK], I[BLK];
+        int32_t pa[BLK], pb[BLK];
+        uint32_t z2[BLK / 2];  // choice words: cell 2t in bits 0..15, cell 2t+1 in bits 16..31
+        int32_t cmprev = NEG_INF;
+        bool c_blk = false, c_prev = false, slow = d > TRACK_MAX_D, slow0 = false;
+        uint32_t hm = 0;  // bit l: Mpre[l] >= Dv[l], then (after the scan) M[l] == Mpre[l]
+        uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
+        const int32_t minit = multi ? INT_MIN : NEG_INF;
+#pragma unroll
+        for (int l = 0; l < BLK; l++) Mpre[l] = Dv[l] = pa[l] = pb[l] = minit;
+#pragma unroll
+        for (int t = 0; t < BLK / 2; t++) z2[t] = 0xffffffffu;
+        if (act) {
+            const uint2 qw = *reinterpret_cast<const uint2*>(qsm + B * BLK);
+            qlo = qw.x;
+            qhi = qw.y;
+            if (i == 0 && b == 0) Mpre[0] = 0;
+        }
+        auto qc_at = [&](int l) { return (int)(((l < 4 ? qlo : qhi) >> (8 * (l & 3))) & 255u); };
+        if (act) {
+            for (int k = 0; k < d; k++) {
+                const int4 ek = er[k];
+                const int pBs = ek.x & 0xffff, pBe = ek.x >> 16;
+                const int32_t* src = a.rs + ek.y;
+                const int pbase = ek.w & 255;
+                const PredMask mk = pred_mask(B, pBs, pBe);
+                int32_t mprev = NEG_INF;
+                if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                if (mk.blk_in) {
+                    int32_t Mb[BLK], Db[BLK];
+                    load_block16(src + (B - pBs) * 16, Mb, Db);
+                    if (multi) {
+                        const uint32_t pos = ((uint32_t)ek.z >> 16) & 15u;  // exact when d <= TRACK_MAX_D
+                        const uint32_t p1 = (ek.w & 256) ? pos : Y_NONE;
+#pragma unroll
+                        for (int l = 0; l < BLK; l++)
+                            track_d(sc, Mb[l], Db[l], pos, Dv[l], pb[l], z2[l >> 1], 16 * (l & 1));
+                        if (mk.diag) {
+                            // cell 0 of the row's first block reads NEG_INF (the lane quirk); the
+                            // backtrack never takes that term, so it records no position
+                            const bool first = b == 0;
+                            const bool bm0 = pbase == qc_at(0);
+                            track_m(add32(first ? NEG_INF : mprev, bm0 ? sc.match : sc.mismatch), bm0,
+                                    first ? Y_NONE : pos, first ? Y_NONE : p1, Mpre[0], pa[0], z2[0], 0);
+#pragma unroll
+                            for (int l = 1; l < BLK; l++) {
+                                const bool bm = pbase == qc_at(l);
+                                track_m(add32(Mb[l - 1], bm ? sc.match : sc.mismatch), bm, pos, p1, Mpre[l], pa[l],
+                                        z2[l >> 1], 16 * (l & 1));
+                            }
+                        }
+                    } else {
+                        uint8_t qc8[BLK];
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) qc8[l] = (uint8_t)qc_at(l);
+                        pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) { pa[l] = Mb[l]; pb[l] = Db[l]; }
+                    }
+                }
+                if (multi) {
+                    slow |= mk.blk_in && !mk.diag;
+                    slow0 |= mk.prev_in && !(mk.blk_in && mk.diag && b != 0);
+                } else {
+                    cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in;
+                }
+            }
+        }
+        if (multi) {
+            // final maxima, and the choices folded into z (see above)
+#pragma unroll
+            for (int l = 0; l < BLK; l++) {
+                const int sh = 16 * (l & 1);
+                const uint32_t y = (z2[l >> 1] >> sh) & 0xffffu;
+                const int32_t mp = mx(NEG_INF, Mpre[l]);
+                const int32_t dv = mx(NEG_INF, mx(Dv[l], pb[l]));  // Dv: max of M_p + o1, pb: of D_p + e1
+                const bool okO = Dv[l] == dv, okE = pb[l] == dv;
+                uint32_t w = okO ? (y & 15u) : (okE ? (((y >> Y_E) & 15u) | W_DEXT) : Y_NONE);
+                w |= Mpre[l] == mp ? (y & 0x0f00u) : 0x0f00u;
+                w |= pa[l] == mp ? (y & 0xf000u) : 0xf000u;
+                z2[l >> 1] = (z2[l >> 1] & ~(0xffffu << sh)) | (w << sh);
+                Mpre[l] = mp;
+                Dv[l] = dv;
+            }
+        }
+        // prefix max of the scan keys across the warp
+        int32_t agg = INT_MIN;
+#pragma unroll
+        for (int l = 0; l < BLK; l++) {
+            H0[l] = mx(Mpre[l], Dv[l]);
+            if (Mpre[l] >= Dv[l]) hm |= 1u << l;
+            agg = mx(agg, add32(H0[l], -(j0 + l) * sc.e1));
+        }
+        if (!act) agg = INT_MIN;
+        const int32_t incl = warp_incl_max(agg);
+        int32_t P = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) P = INT_MIN;
+        P = mx(P, carryP);
+        const int32_t chunk_total = __shfl_sync(0xffffffffu, incl, 31);
+        if (i == 0) {
+#pragma unroll
+            for (int l = 0; l < BLK; l++) { M[l] = H0[l]; I[l] = NEG_INF; }
+        } else {
+            int32_t run = P;
+#pragma unroll
+            for (int l = 0; l < BLK; l++) {
+                I[l] = add32(sc.o1 + (j0 + l - 1) * sc.e1, run);
+                M[l] = mx(H0[l], I[l]);
+                if (H0[l] < I[l]) hm &= ~(1u << l);
+                run = mx(run, add32(H0[l], -(j0 + l) * sc.e1));
+            }
+        }
+        if (ARGMAX && act) {
+#pragma unroll
+            for (int l = 0; l < BLK; l++)
+                if (M[l] > bestM) { bestM = M[l]; bestJ = j0 + l; }  // first maximum of the row
+        }
+        const int32_t upM = __shfl_up_sync(0xffffffffu, M[BLK - 1], 1);
+        const int32_t upI = __shfl_up_sync(0xffffffffu, I[BLK - 1], 1);
+        const int32_t Ml0 = lane > 0 ? upM : carryM, Il0 = lane > 0 ? upI : carryI;
+        const int32_t nextM = __shfl_sync(0xffffffffu, M[BLK - 1], 31);
+        const int32_t nextI = __shfl_sync(0xffffffffu, I[BLK - 1], 31);
+        if (act) {
+            if (!multi) {
+                uint32_t lo = 0, hi = 0;
+#pragma unroll
+                for (int l = 0; l < BLK; l++) {
+                    const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                    uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
+                    if (d == 1) {
+                        const bool inr = l == 0 ? c_prev : c_blk;
+                        const int32_t mv = l == 0 ? cmprev : pa[l > 0 ? l - 1 : 0];
+                        const bool bm = cur.pbase == qc_at(l);
+                        const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                        if (eqM) r |= R_M4;
+                        if (eqM && bm && cur.w1ok) r |= R_M1;
+                        if (c_blk && Dv[l] == add32(pa[l], sc.o1)) r |= R_DOPEN;
+                        else if (c_blk && Dv[l] == add32(pb[l], sc.e1)) r |= R_DEXT;
+                    }
+                    if (l < 4) lo |= r << (8 * l);
+                    else hi |= r << (8 * (l - 4));
+                }
+                *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
+            } else {
+                uint32_t r[BLK];
+                if (!slow) {
+                    uint32_t c0 = 0x01ff01ffu;
+                    if (slow0) {
+                        // cell 0 by the backtrack's own test, over every predecessor
+                        const int qc = qc_at(0);
+                        for (int k = 0; k < d; k++) {
+                            const int4 ek = er[k];
+                            const int pBs = ek.x & 0xffff, pBe = ek.x >> 16;
+                            if (!(B - 1 >= pBs && B - 1 <= pBe - 2)) continue;  // prev_in
+                            const int32_t mv = a.rs[ek.y + (B - 1 - pBs) * 16 + 7];
+                            const uint32_t pos = (uint32_t)ek.z >> 16;
+                            const bool bm = (ek.w & 255) == qc;
+                            if (M[0] != add32(mv, bm ? sc.match : sc.mismatch)) continue;
+                            if ((c0 >> 16) == 511u) c0 = (c0 & 0xffffu) | (pos << 16);
+                            if (bm && (c0 & 0xffffu) == 511u) c0 = (c0 & 0xffff0000u) | ((ek.w & 256) ? pos : 510u);
+                        }
+                    }
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                        const uint32_t own = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
+                        const uint32_t w = (z2[l >> 1] >> (16 * (l & 1))) & 0xffffu;
+                        const bool h = (hm >> l) & 1u;
+                        const uint32_t n4 = (w >> Y_4) & 15u, n1 = (w >> Y_1) & 15u, nd = w & 15u;
+                        uint32_t m4 = (h && n4 != Y_NONE) ? n4 : W_NONE;
+                        uint32_t m1 = (h && n1 != Y_NONE) ? n1 : W_NONE;
+                        if (l == 0 && slow0) {
+                            m1 = c0 & 0xffffu;
+                            if (m1 == 510u) m1 = W_NONE;
+                            m4 = c0 >> 16;
+                        }
+                        const uint32_t dd = nd != Y_NONE ? nd : W_NONE;
+                        r[l] = own | (w & W_DEXT) | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
+                    }
+                } else {
+                    // every choice by the backtrack's own test, over every predecessor
+                    uint32_t cm[BLK], cd[BLK];
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) cm[l] = cd[l] = 0x01ff01ffu;
+                    for (int k = 0; k < d; k++) {
+                        const int4 ek = er[k];
+                        const int pBs = ek.x & 0xffff, pBe = ek.x >> 16;
+                        const int32_t* src = a.rs + ek.y;
+                        const PredMask mk = pred_mask(B, pBs, pBe);
+                        if (!(mk.blk_in || mk.prev_in)) continue;
+                        const uint32_t pos = (uint32_t)ek.z >> 16;
+                        const int pbase = ek.w & 255;
+                        const uint32_t m1v = (ek.w & 256) ? pos : 510u;
+                        int32_t Mb[BLK], Db[BLK];
+                        int32_t mprev = NEG_INF;
+                        if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
+                        if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
+                        else {
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                        }
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) {
+                            const bool inr = l == 0 ? mk.prev_in : mk.blk_in;
+                            const int32_t mv = l == 0 ? mprev : Mb[l > 0 ? l - 1 : 0];
+                            const bool bm = pbase == qc_at(l);
+                            const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                            if (eqM && (cm[l] >> 16) == 511u) cm[l] = (cm[l] & 0xffffu) | (pos << 16);
+                            if (eqM && bm && (cm[l] & 0xffffu) == 511u) cm[l] = (cm[l] & 0xffff0000u) | m1v;
+                            if (mk.blk_in) {
+                                if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
+                                    cd[l] = (cd[l] & 0xffff0000u) | pos;
+                                if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
+                                    cd[l] = (cd[l] & 0xffffu) | (pos << 16);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int l = 0; l < BLK; l++) {
+                        const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
+                        uint32_t w = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
+                        uint32_t m1 = cm[l] & 0xffffu, m4 = cm[l] >> 16;
+                        if (m1 == 510u) m1 = W_NONE;
+                        uint32_t dd = cd[l] & 0xffffu;
+                        if (dd == 511u) {
+                            dd = cd[l] >> 16;
+                            if (dd != 511u) w |= W_DEXT;
+                        }
+                        r[l] = w | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
+                    }
+                }
+                uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);
+                tdst[0] = make_uint4(r[0], r[1], r[2], r[3]);
+                tdst[1] = make_uint4(r[4], r[5], r[6], r[7]);
+            }
+            store_block16(dst + b * 16, M, Dv);
+        }
+        carryP = mx(carryP, chunk_total);
+        carryM = nextM;
+        carryI = nextI;
+    }
+}
+
 __device__ void dp_fill_warp_static(const DpArgs& a, const RowDesc* __restrict__ desc, const int4* __restrict__ erec,
                                     int32_t* ring, int RB, const uint8_t* qsm, unsigned char* stage, int lane) {
     const int n = a.v.n, m = a.qlen + 1;
@@ -1238,8 +1515,8 @@ __device__ void dp_fill_warp_dyn(const DpArgs& a, int4* __restrict__ erec, const
         }
         int32_t bestM = INT_MIN;
         int bestJ = 0;
-        if (adaptive) fill_row<true, true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
-        else fill_row<false, true>(a, cur, er, nullptr, 0, qsm, i, lane, bestM, bestJ);
+        if (adaptive) fill_row_dyn<true>(a, cur, er, qsm, i, lane, bestM, bestJ);
+        else fill_row_dyn<false>(a, cur, er, qsm, i, lane, bestM, bestJ);
         cells += (int64_t)bn * BLK;
         ecells += (int64_t)bn * BLK * d;
         if (adaptive && i >= 1) {

@@ -259,6 +259,65 @@ PB_HD uint32_t encode_wide(uint32_t own, const FlagAcc& a, int l, int ind) {
     return r | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
 }
 
+// One-pass record choices of a multi-predecessor row (the batch kernel's
+// adaptive fill). The predecessors arrive in the backtrack's priority order
+// (in_weight descending, in-list position ascending), so each choice is the
+// FIRST predecessor whose term equals the cell's final value. Per cell and
+// per kind of term the fill keeps the running maximum of the terms seen so
+// far and, in a 4-bit field, the in-list position of the first predecessor
+// that reached it (a strict > keeps the first on ties):
+//   y bits 0..3   dopen: first p with M_p + o1 at the max of those terms
+//          4..7   dext : first p with D_p + e1 at the max of those terms
+//          8..11  m4   : first p with M_p[j-1] + s at the diagonal max
+//         12..15  m1   : first matching p (base_p == q[j-1]) at the max of
+//                        the matching diagonal terms; 15 when that p fails
+//                        the in_weight >= ind/10 rule (a later p may not
+//                        take its place, src/align.cpp:1592-1604)
+// 15 = none. A choice stands iff its maximum equals the final value (D for
+// dopen/dext, M == Mpre for m4/m1), which is exactly "the first p whose term
+// equals the final value". Positions must fit 4 bits: rows with more than
+// TRACK_MAX_D in-window predecessors take the kernel's second pass instead.
+constexpr int TRACK_MAX_D = 15;
+constexpr uint32_t Y_NONE = 15u, Y_INIT = 0xffffu;
+enum { Y_O = 0, Y_E = 4, Y_4 = 8, Y_1 = 12 };
+
+PB_HD uint32_t y_set(uint32_t y, int sh, uint32_t v) { return (y & ~(15u << sh)) | (v << sh); }
+
+// Vertical terms of one predecessor at one cell (the caller applies the
+// vertical mask).
+// The fields sit at bit `sh` of y (0, or 16 for the second cell of a pair
+// that shares one register).
+PB_HD void track_d(const Scoring& s, int32_t mb, int32_t db, uint32_t pos, int32_t& mO, int32_t& mE, uint32_t& y,
+                   int sh = 0) {
+    const int32_t co = add32(mb, s.o1), ce = add32(db, s.e1);
+    if (co > mO) { mO = co; y = y_set(y, sh + Y_O, pos); }
+    if (ce > mE) { mE = ce; y = y_set(y, sh + Y_E, pos); }
+}
+
+// Diagonal term `cand` of one predecessor at one cell (the caller applies the
+// diagonal mask); pos4 / pos1 are the values recorded for m4 / m1 (Y_NONE
+// where the backtrack never tests this term).
+PB_HD void track_m(int32_t cand, bool bm, uint32_t pos4, uint32_t pos1, int32_t& mM, int32_t& m1, uint32_t& y,
+                   int sh = 0) {
+    if (cand > mM) { mM = cand; y = y_set(y, sh + Y_4, pos4); }
+    if (bm && cand > m1) { m1 = cand; y = y_set(y, sh + Y_1, pos1); }
+}
+
+// The 4-byte record of one cell from the one-pass choices: own = own_flags,
+// hm = (final M == Mpre), Mpre / Dv = the cell's diagonal / vertical maxima
+// (clamped at NEG_INF as the fill initialises them).
+PB_HD uint32_t track_record(uint32_t own, bool hm, int32_t Mpre, int32_t Dv, int32_t mM, int32_t m1, int32_t mO,
+                            int32_t mE, uint32_t y) {
+    const uint32_t n4 = (y >> Y_4) & 15u, n1 = (y >> Y_1) & 15u, nO = (y >> Y_O) & 15u, nE = (y >> Y_E) & 15u;
+    const uint32_t m4v = (hm && mM == Mpre && n4 != Y_NONE) ? n4 : W_NONE;
+    const uint32_t m1v = (hm && m1 == Mpre && n1 != Y_NONE) ? n1 : W_NONE;
+    const bool okO = mO == Dv, okE = mE == Dv;
+    uint32_t r = own & 15u;
+    const uint32_t dd = okO ? nO : (okE ? nE : W_NONE);
+    if (!okO && okE) r |= W_DEXT;
+    return r | (m1v << W_M1_SHIFT) | (m4v << W_M4_SHIFT) | (dd << W_D_SHIFT);
+}
+
 // Decoded view of one record for the backtrack.
 struct Rec {
     bool eqMD, eqMI, iopen, iext;

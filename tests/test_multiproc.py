@@ -1,22 +1,41 @@
-"""The multi-GPU bench path, exercised on CPU with two gloo ranks.
+"""The multi-GPU path, exercised on CPU with two gloo ranks.
 
-bench.py shards windows across ranks with no collective on the data path;
-torch.distributed only provides the barrier and the max / sum over ranks of
-the measured times and counters. This runs that logic with world size 2 on
-the gloo backend (no GPU) and checks the reductions, the per-rank shards and
-the whole-job rate.
+bench.py (and poa_batch_consensus_multi in the library) split ONE window set
+over the ranks by cost (poa_batch_partition), run each share with no
+collective on the data path, and gather the per-window results in input
+order; torch.distributed gives the barrier, the max / sum over ranks of the
+measured times and counters, and the gather. Here two gloo ranks (no GPU)
+run that logic on a real window list, each computing its share's consensus
+with the CPU restatement in oracle/ standing in for its device, and the
+gathered result must equal a single process's over the whole list.
 """
 import os
 import socket
+import subprocess
+import tempfile
 
 import pytest
 import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "build", "poa_oracle")
 
 
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
+
+
+def _consensus(ws, windows):
+    from poa_b200 import synth
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        for w in windows:
+            fa = os.path.join(d, "w.fa")
+            synth.write_fasta(fa, ws.window_reads(int(w)))
+            out.append(subprocess.run([ORACLE, fa], capture_output=True, check=True).stdout)
+    return out
 
 
 def _worker(rank, world, port, out):
@@ -30,22 +49,28 @@ def _worker(rank, world, port, out):
         t = 1.0 + rank                      # rank 1 is the slow one
         t_max = D.max(t)
         failed = D.sum(rank)                # counters add up
-        ws = synth.polishing_windows(seed=bench.shard_seed(rank), n_windows=3)
-        first = ws.window_reads(0)[0]
-        out[rank] = (t_max, failed, ws.n_windows, first[:32])
+        ws = synth.polishing_windows(seed=43, n_windows=12)
+        mine = bench.rank_windows(ws, world, rank)
+        cons = _consensus(ws, mine)
+        gathered = bench.gather_in_order(D, mine, cons, ws.n_windows)
+        out[rank] = (t_max, failed, [int(w) for w in mine], gathered)
     finally:
         D.close()
 
 
-def test_two_gloo_ranks():
+def test_two_gloo_ranks_share_one_window_set(oracle_bin):
     world, port = 2, _free_port()
     mgr = mp.Manager()
     out = mgr.dict()
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
-    (t0, f0, n0, r0), (t1, f1, n1, r1) = out[0], out[1]
+    (t0, f0, m0, g0), (t1, f1, m1, g1) = out[0], out[1]
     assert t0 == t1 == 2.0          # both ranks see the slowest rank's time
     assert f0 == f1 == 1            # 0 + 1
-    assert n0 == n1 == 3            # weak scaling: the same work per rank
-    assert r0 != r1                 # distinct shards
+    assert sorted(m0 + m1) == list(range(12)) and not set(m0) & set(m1)  # every window once
+    assert m0 and m1                # both ranks have work
+    from poa_b200 import synth
+    ws = synth.polishing_windows(seed=43, n_windows=12)
+    want = _consensus(ws, range(12))
+    assert g0 == g1 == want         # gathered in input order, equal to one process's results
     import bench
-    assert bench.whole_job_rate(world, n0, 5, t0) == pytest.approx(2 * 3 * 5 / 2.0)
+    assert bench.whole_job_rate(12, 5, t0) == pytest.approx(12 * 5 / 2.0)

@@ -296,6 +296,11 @@ int poa_prop_train(poa_proposer* p, const float* X, const float* Y, int64_t n, i
                    float lr, uint64_t seed, float* losses);
 /* Raw predictions Y [n][4] for features X [n][32][8]. */
 int poa_prop_predict(poa_proposer* p, const float* X, int64_t n, float* Y);
+/* Loss (mean squared error of the standardised outputs) and the gradient of
+ * every parameter (poa_prop_nweights() - 12 floats, the parameter layout of
+ * poa_prop_get_weights) for one batch of 1..4096 reads, without an update:
+ * the backward kernels of one training step. */
+int poa_prop_gradient(poa_proposer* p, const float* X, const float* Y, int64_t n, float* grad, float* loss);
 /* Features of every read of the uploaded batch: n_reads * 32 * 8 floats. */
 int poa_batch_features(poa_ctx* ctx, poa_proposer* p, float* X, int64_t cap);
 /* Features, prediction and per-window plan on the device, then

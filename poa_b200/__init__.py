@@ -136,6 +136,8 @@ def lib() -> ctypes.CDLL:
     L.poa_prop_train.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                  ctypes.c_int32, ctypes.c_float, ctypes.c_uint64, ctypes.c_void_p]
     L.poa_prop_predict.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+    L.poa_prop_gradient.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                    ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
     L.poa_batch_features.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
     L.poa_batch_propose.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.poa_batch_use_proposer.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
@@ -415,6 +417,17 @@ class Proposer:
         Y = np.zeros((X.shape[0], PROP_OUT), dtype=np.float32)
         self._check(lib().poa_prop_predict(self._h, X.ctypes.data, X.shape[0], Y.ctypes.data))
         return Y
+
+    def gradient(self, X, Y):
+        """(loss, parameter gradient) of one batch (1..4096 reads), no update."""
+        import numpy as np
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        g = np.zeros(self.nweights() - 12, dtype=np.float32)
+        loss = ctypes.c_float()
+        self._check(lib().poa_prop_gradient(self._h, X.ctypes.data, Y.ctypes.data, X.shape[0], g.ctypes.data,
+                                            ctypes.byref(loss)))
+        return loss.value, g
 
 
 class PinnedArray:

@@ -4,11 +4,15 @@
 // fixed capacities: per node base, par_id, aligned_node[5], in-degree count,
 // rank and the heads/tails of two singly linked edge lists (in-list and
 // out-list, kept in insertion order exactly like node_t's vectors); per edge
-// its endpoints, weight and the next links of both lists. Fusion
-// (src/graph.cpp:170-235), the LIFO topological sort with hlen/tlen
-// (src/graph.cpp:21-128) and the consensus (src/graph.cpp:294-351) are the
-// reference's sequential algorithms, run by lane 0; the window view of the
-// DP rows, the shifted query and the DP fill itself use the whole warp.
+// its endpoints, weight and the next links of both lists. One warp runs a
+// window: fusion (src/graph.cpp:170-235) is warp-parallel with stamp-based
+// conflict detection and a sequential fallback (dg_fuse_warp / dg_fuse_seq);
+// the LIFO topological sort (src/graph.cpp:21-128) runs its Kahn loop over a
+// shared-memory CSR copy, with hlen/tlen as depths by pointer jumping over
+// the warp; the window view of the DP rows, the shifted query, the fill and
+// the static-band backtrack use the whole warp; the adaptive-band backtrack
+// and the consensus (src/graph.cpp:294-351) are the reference's sequential
+// walks, run by lane 0.
 #include "batch.h"
 #include "proposer.h"
 

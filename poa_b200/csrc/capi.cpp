@@ -472,6 +472,18 @@ int poa_prop_train(poa_proposer* p, const float* X, const float* Y, int64_t n, i
     return POA_OK;
 }
 
+int poa_prop_gradient(poa_proposer* p, const float* X, const float* Y, int64_t n, float* grad, float* loss) {
+    if (!p || !X || !Y || !grad) return prop_fail(p, POA_BAD_ARG, "null argument");
+    if (n <= 0 || n > 4096) return prop_fail(p, POA_BAD_ARG, "gradient batch must hold 1..4096 reads");
+    try {
+        const float l = p->prop->gradient(X, Y, n, grad);
+        if (loss) *loss = l;
+    } catch (const std::exception& e) {
+        return prop_fail(p, POA_CUDA, e.what());
+    }
+    return POA_OK;
+}
+
 int poa_prop_predict(poa_proposer* p, const float* X, int64_t n, float* Y) {
     if (!p || (n > 0 && (!X || !Y)) || n < 0) return prop_fail(p, POA_BAD_ARG, "bad argument");
     if (n == 0) return POA_OK;

@@ -615,7 +615,6 @@ float Proposer::train(const float* X, const float* Y, int64_t n, int epochs, int
     ensure(batch);
     Act a;
     act_layout(cap_, &a, (char*)d_act_);
-    const bf16* W = (const bf16*)d_wb_;
     std::vector<int32_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0);
     std::mt19937_64 rng(seed);
@@ -628,37 +627,8 @@ float Proposer::train(const float* X, const float* Y, int64_t n, int epochs, int
         int nbatches = 0;
         for (int64_t b0 = 0; b0 < n; b0 += batch) {
             const int nb = (int)std::min<int64_t>(batch, n - b0);
-            const int64_t R = (int64_t)nb * T;
             k_gather<<<grid_of((int64_t)nb * T * PROP_CIN), 256, 0, s>>>(dX, dY, dIdx + b0, nb, d_extra_, a.x0, a.yt);
-            forward(nullptr, nb, s);
-            k_loss<<<1, 256, 0, s>>>(a.o, a.yt, a.dob, nb, a.loss);
-            // output layer
-            gemm<true, false>(s, a.dob, PROP_OUT, a.z, PROP_CH, d_g_ + OW5, nullptr, PROP_CH, PROP_OUT, PROP_CH, nb,
-                              nullptr, 0);
-            k_colsum<<<PROP_OUT, 256, 0, s>>>(a.dob, nb, PROP_OUT, d_g_ + OB5);
-            gemm<false, false>(s, a.dob, PROP_OUT, W + OW5, PROP_CH, a.dz, nullptr, PROP_CH, nb, PROP_CH, PROP_OUT,
-                               nullptr, 0);
-            k_relu_mask<<<grid_of((int64_t)nb * PROP_CH), 256, 0, s>>>(a.dz, a.z, a.dzb, (int64_t)nb * PROP_CH);
-            // hidden dense layer
-            gemm<true, false>(s, a.dzb, PROP_CH, a.h, PROP_CH, d_g_ + OW4, nullptr, PROP_CH, PROP_CH, PROP_CH, nb,
-                              nullptr, 0);
-            k_colsum<<<PROP_CH, 256, 0, s>>>(a.dzb, nb, PROP_CH, d_g_ + OB4);
-            gemm<false, false>(s, a.dzb, PROP_CH, W + OW4, PROP_CH, a.dh, nullptr, PROP_CH, nb, PROP_CH, PROP_CH,
-                               nullptr, 0);
-            k_unpool_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dh, a.y3, a.dy3, nb);
-            // conv 3
-            gemm<true, false>(s, a.dy3, PROP_CH, a.xc3, KC, d_g_ + OW3, nullptr, KC, PROP_CH, KC, R, nullptr, 0);
-            k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy3, R, PROP_CH, d_g_ + OB3);
-            gemm<false, false>(s, a.dy3, PROP_CH, W + OW3, KC, a.dxc, nullptr, KC, R, KC, PROP_CH, nullptr, 0);
-            k_col2im_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dxc, a.y2, a.dy2, R, PROP_CH);
-            // conv 2
-            gemm<true, false>(s, a.dy2, PROP_CH, a.xc2, KC, d_g_ + OW2, nullptr, KC, PROP_CH, KC, R, nullptr, 0);
-            k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy2, R, PROP_CH, d_g_ + OB2);
-            gemm<false, false>(s, a.dy2, PROP_CH, W + OW2, KC, a.dxc, nullptr, KC, R, KC, PROP_CH, nullptr, 0);
-            k_col2im_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dxc, a.y1, a.dy1, R, PROP_CH);
-            // conv 1 (no input gradient)
-            gemm<true, false>(s, a.dy1, PROP_CH, a.xc1, KC1, d_g_ + OW1, nullptr, KC1, PROP_CH, KC1, R, nullptr, 0);
-            k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy1, R, PROP_CH, d_g_ + OB1);
+            loss_and_gradient(nb, s);
             step++;
             const float b1 = 0.9f, b2 = 0.999f;
             k_adam<<<grid_of(PROP_NPARAM), 256, 0, s>>>(d_w_, (bf16*)d_wb_, d_g_, d_m_, d_v_, PROP_NPARAM, lr, b1, b2,
@@ -676,6 +646,76 @@ float Proposer::train(const float* X, const float* Y, int64_t n, int epochs, int
     cudaFree(dY);
     cudaFree(dIdx);
     return last;
+}
+
+// Loss and parameter gradient of one batch whose BF16 inputs are in act.x0 and
+// standardised targets in act.yt: forward, MSE (summed into act.loss), then
+// the backward GEMMs, col2im / unpooling with the ReLU masks and the bias
+// column sums into d_g_.
+void Proposer::loss_and_gradient(int nb, void* stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    Act a;
+    act_layout(cap_, &a, (char*)d_act_);
+    const bf16* W = (const bf16*)d_wb_;
+    const int64_t R = (int64_t)nb * T;
+    forward(nullptr, nb, s);
+    k_loss<<<1, 256, 0, s>>>(a.o, a.yt, a.dob, nb, a.loss);
+    // output layer
+    gemm<true, false>(s, a.dob, PROP_OUT, a.z, PROP_CH, d_g_ + OW5, nullptr, PROP_CH, PROP_OUT, PROP_CH, nb,
+                      nullptr, 0);
+    k_colsum<<<PROP_OUT, 256, 0, s>>>(a.dob, nb, PROP_OUT, d_g_ + OB5);
+    gemm<false, false>(s, a.dob, PROP_OUT, W + OW5, PROP_CH, a.dz, nullptr, PROP_CH, nb, PROP_CH, PROP_OUT,
+                       nullptr, 0);
+    k_relu_mask<<<grid_of((int64_t)nb * PROP_CH), 256, 0, s>>>(a.dz, a.z, a.dzb, (int64_t)nb * PROP_CH);
+    // hidden dense layer
+    gemm<true, false>(s, a.dzb, PROP_CH, a.h, PROP_CH, d_g_ + OW4, nullptr, PROP_CH, PROP_CH, PROP_CH, nb,
+                      nullptr, 0);
+    k_colsum<<<PROP_CH, 256, 0, s>>>(a.dzb, nb, PROP_CH, d_g_ + OB4);
+    gemm<false, false>(s, a.dzb, PROP_CH, W + OW4, PROP_CH, a.dh, nullptr, PROP_CH, nb, PROP_CH, PROP_CH,
+                       nullptr, 0);
+    k_unpool_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dh, a.y3, a.dy3, nb);
+    // conv 3
+    gemm<true, false>(s, a.dy3, PROP_CH, a.xc3, KC, d_g_ + OW3, nullptr, KC, PROP_CH, KC, R, nullptr, 0);
+    k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy3, R, PROP_CH, d_g_ + OB3);
+    gemm<false, false>(s, a.dy3, PROP_CH, W + OW3, KC, a.dxc, nullptr, KC, R, KC, PROP_CH, nullptr, 0);
+    k_col2im_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dxc, a.y2, a.dy2, R, PROP_CH);
+    // conv 2
+    gemm<true, false>(s, a.dy2, PROP_CH, a.xc2, KC, d_g_ + OW2, nullptr, KC, PROP_CH, KC, R, nullptr, 0);
+    k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy2, R, PROP_CH, d_g_ + OB2);
+    gemm<false, false>(s, a.dy2, PROP_CH, W + OW2, KC, a.dxc, nullptr, KC, R, KC, PROP_CH, nullptr, 0);
+    k_col2im_relu<<<grid_of(R * PROP_CH), 256, 0, s>>>(a.dxc, a.y1, a.dy1, R, PROP_CH);
+    // conv 1 (no input gradient)
+    gemm<true, false>(s, a.dy1, PROP_CH, a.xc1, KC1, d_g_ + OW1, nullptr, KC1, PROP_CH, KC1, R, nullptr, 0);
+    k_colsum<<<PROP_CH, 256, 0, s>>>(a.dy1, R, PROP_CH, d_g_ + OB1);
+    cuda_check(cudaGetLastError(), "proposer backward");
+}
+
+float Proposer::gradient(const float* X, const float* Y, int64_t n, float* grad) {
+    cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+    if (n <= 0 || n > 4096) throw std::invalid_argument("proposer: gradient batch must hold 1..4096 reads");
+    float *dX = nullptr, *dY = nullptr;
+    int32_t* dIdx = nullptr;
+    cuda_check(cudaMalloc(&dX, 4 * (size_t)n * T * PROP_CIN), "cudaMalloc(grad X)");
+    cuda_check(cudaMalloc(&dY, 4 * (size_t)n * PROP_OUT), "cudaMalloc(grad Y)");
+    cuda_check(cudaMalloc(&dIdx, 4 * (size_t)n), "cudaMalloc(grad idx)");
+    std::vector<int32_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0);
+    cuda_check(cudaMemcpy(dX, X, 4 * (size_t)n * T * PROP_CIN, cudaMemcpyHostToDevice), "H2D X");
+    cuda_check(cudaMemcpy(dY, Y, 4 * (size_t)n * PROP_OUT, cudaMemcpyHostToDevice), "H2D Y");
+    cuda_check(cudaMemcpy(dIdx, idx.data(), 4 * (size_t)n, cudaMemcpyHostToDevice), "H2D idx");
+    ensure(n);
+    Act a;
+    act_layout(cap_, &a, (char*)d_act_);
+    cuda_check(cudaMemset(a.loss, 0, 4), "memset loss");
+    k_gather<<<grid_of(n * T * PROP_CIN), 256>>>(dX, dY, dIdx, (int)n, d_extra_, a.x0, a.yt);
+    loss_and_gradient((int)n, nullptr);
+    float loss = 0.f;
+    cuda_check(cudaMemcpy(grad, d_g_, 4 * (size_t)PROP_NPARAM, cudaMemcpyDeviceToHost), "D2H grad");
+    cuda_check(cudaMemcpy(&loss, a.loss, 4, cudaMemcpyDeviceToHost), "D2H loss");
+    cudaFree(dX);
+    cudaFree(dY);
+    cudaFree(dIdx);
+    return loss;
 }
 
 constexpr int64_t PREDICT_CHUNK = 4096;

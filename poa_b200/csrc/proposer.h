@@ -66,6 +66,10 @@ class Proposer {
     // mean loss; per-epoch losses go to `losses` (may be null).
     float train(const float* X, const float* Y, int64_t n, int epochs, int batch, float lr, uint64_t seed,
                 float* losses);
+    // Loss (mean squared error on the standardised targets) and the gradient
+    // of every parameter (PROP_NPARAM floats) for one batch of n <= 4096 reads,
+    // without an update: the backward kernels the training step runs.
+    float gradient(const float* X, const float* Y, int64_t n, float* grad);
     // Inference on host arrays: Y [n][PROP_OUT] raw (de-standardised) outputs.
     void predict_host(const float* X, int64_t n, float* Y);
     // Inference on device arrays (stream order on `stream`).
@@ -98,6 +102,7 @@ class Proposer {
     GraphKey graph_key_{};
     void ensure(int64_t batch_reads);
     void forward(const float* dX, int64_t n, void* stream);
+    void loss_and_gradient(int nb, void* stream);
     void upload_bf16(void* stream);
     int device_;
     std::vector<float> host_w_;

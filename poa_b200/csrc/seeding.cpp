@@ -10,6 +10,13 @@
 // global chain of local chains with the minimum-spacing filter
 // (src/lchain.cpp:269-386, from abPOA). Float arithmetic follows the same
 // expressions in the same order (IEEE single, no contraction).
+//
+// Lineage and licences: the algorithms restated here come, through minipoa
+// (MIT, Copyright (c) 2025 Haodong Liu), from minimap2 (MIT, Heng Li; the
+// sketch, mg_chain_bk_end, comput_sc, mg_lchain_dp and mg_log2) and klib's
+// ksort.h (MIT, Copyright (c) 2008, 2011 Attractive Chaos; the radix sort),
+// and from abPOA (MIT, Yan Gao; the chain of local chains). Bit-exact anchors
+// need their exact steps, tie orders and float evaluation order.
 #include "seeding.h"
 
 #include <algorithm>

@@ -1,5 +1,9 @@
 // sketch.h - the minimizer k-mer hash shared by the host seeding (-S) and the
 // device feature kernel of the band proposer.
+//
+// The hash is Thomas Wang's 64-bit integer hash as minimap2 (MIT, Heng Li)
+// and minipoa (src/minimizer.cpp:11-21; MIT, Copyright (c) 2025 Haodong Liu)
+// use it; identical minimizers need the identical function.
 #pragma once
 #include <stdint.h>
 

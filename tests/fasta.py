@@ -1,4 +1,13 @@
 """Small readers for the test fixtures (FASTA and per-call dumps)."""
+import os
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_input(case):
+    """Input FASTA of a manifest case: its own <case>.fa, or the shared file it
+    names in "input" (the reference's data/mtDNA.fasta serves four cases)."""
+    return os.path.join(GOLD, case.get("input", case["case"] + ".fa"))
 
 
 def read_records(path):

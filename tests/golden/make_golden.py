@@ -7,6 +7,8 @@ reference's own sources into ``oracle/_ref/``):
     python tests/golden/make_golden.py --fullsize   # md5 of full-size runs
     python tests/golden/make_golden.py --windows    # per-window manifests of the
                                                     # full batched window sets
+    python tests/golden/make_golden.py --fixtures   # the reference's own data
+                                                    # file (POA_REF_DIR/data)
 
 For every case it writes ``<case>.fa`` (seeded synthetic input),
 ``<case>.out`` (the reference CLI's stdout, byte for byte: consensus, MSA or GFA) and, where the case
@@ -197,11 +199,48 @@ def window_manifests(only=None):
         print(name, head["reference_seconds"], "s")
 
 
+# The reference's only fixture, data/mtDNA.fasta (393 HVS-II control-region
+# reads), with the modes its README runs plus -r 2 and -B; copied into
+# mtdna.fa and shared by the four cases ("input" in the manifest). Not
+# covered: `-S -t 12 -r1` (the README's second command) faults in the
+# reference on this file (segmentation fault), so it has no output to match.
+REF_FIXTURES = [("mtdna_cons", []), ("mtdna_msa", ["-r", "1"]), ("mtdna_gfa", ["-r", "2"]),
+                ("mtdna_adaptive", ["-B"])]
+
+
+def reference_fixtures():
+    import shutil
+    ref_dir = os.environ.get("POA_REF_DIR", "/root/reference")
+    src = os.path.join(ref_dir, "data", "mtDNA.fasta")
+    dst = os.path.join(HERE, "mtdna.fa")
+    shutil.copyfile(src, dst)
+    with open(os.path.join(HERE, "manifest.json")) as fh:
+        manifest = [c for c in json.load(fh) if not c["case"].startswith("mtdna_")]
+    _, seqs = fasta_read(dst)
+    for name, opts in REF_FIXTURES:
+        res = subprocess.run([REF_BIN, dst] + opts, capture_output=True, check=True)
+        with open(os.path.join(HERE, name + ".out"), "wb") as fh:
+            fh.write(res.stdout)
+        manifest.append({"case": name, "opts": opts, "nseq": len(seqs), "dump": False, "input": "mtdna.fa"})
+    with open(os.path.join(HERE, "manifest.json"), "w") as fh:
+        json.dump(manifest, fh, indent=1)
+    print(f"{len(REF_FIXTURES)} reference fixture cases written")
+
+
+def fasta_read(path):
+    sys.path.insert(0, ROOT)
+    from tests import fasta
+    return fasta.read(path)
+
+
 def main():
     if not (os.path.exists(REF_BIN) and os.path.exists(HARNESS)):
         sys.exit("build the reference first: make -C oracle ref")
     if "--fullsize" in sys.argv:
         fullsize()
+        return
+    if "--fixtures" in sys.argv:
+        reference_fixtures()
         return
     if "--windows" in sys.argv:
         window_manifests([a for a in sys.argv[1:] if not a.startswith("--")])

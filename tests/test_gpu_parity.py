@@ -25,7 +25,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
 def test_golden(case):
-    fa = os.path.join(GOLD, case["case"] + ".fa")
+    fa = fasta.golden_input(case)
     _, seqs = fasta.read(fa)
     params = poa_b200.Params.from_cli(case["opts"])
     with poa_b200.Context(params) as ctx:

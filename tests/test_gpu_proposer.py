@@ -110,3 +110,52 @@ def test_undersized_plan_falls_back_exactly():
         s1 = ctx.batch_stats()
     assert cons1 == cons0 and st1 == st0
     assert s1["fallback"] == ws.n_windows
+
+
+# ---- the network against its NumPy restatement (tests/proposer_net.py) ----
+from tests import proposer_net as net  # noqa: E402
+
+
+def _check_forward(prop, w, X):
+    got = prop.predict(X)
+    want = net.predict(w, X, use_bf16=True)
+    scale = np.std(want, axis=0) + 1e-3
+    # same BF16 rounding points, float32 accumulation in a different order: a
+    # few activations may round to the neighbouring BF16 value
+    assert np.all(np.abs(got - want) <= 2e-2 * scale[None, :]), np.max(np.abs(got - want) / scale[None, :])
+    assert np.median(np.abs(got - want) / scale[None, :]) < 2e-3
+
+
+def test_forward_pass_matches_numpy_committed_weights():
+    prop = poa_b200.Proposer(weights=poa_b200.PROP_WEIGHTS)
+    w = prop.get_weights().astype(np.float64)
+    ws = _feature_windows()
+    with poa_b200.Context(poa_b200.Params.from_cli(["-B"])) as ctx:
+        ctx.batch_upload(ws)
+        X = ctx.batch_features(prop)
+    _check_forward(prop, w, X)
+
+
+def test_forward_pass_matches_numpy_random_weights():
+    w, X, _ = net.random_problem(7, 300)
+    prop = poa_b200.Proposer()
+    prop.set_weights(w.astype(np.float32))
+    _check_forward(prop, prop.get_weights().astype(np.float64), X.astype(np.float32))
+
+
+@pytest.mark.parametrize("n", [1, 64, 300])
+def test_backward_kernels_match_numpy_gradient(n):
+    w, X, Y = net.random_problem(11 + n, n)
+    prop = poa_b200.Proposer()
+    prop.set_weights(w.astype(np.float32))
+    w32 = prop.get_weights().astype(np.float64)
+    loss, g = prop.gradient(X.astype(np.float32), Y.astype(np.float32))
+    want_loss, want = net.loss_and_gradient(w32, X.astype(np.float32), Y.astype(np.float32), use_bf16=True)
+    assert abs(loss - want_loss) <= 1e-3 * abs(want_loss) + 1e-6
+    o = 0
+    for name, shape in net.SHAPES:
+        k = int(np.prod(shape))
+        a, b = g[o:o + k].astype(np.float64), want[o:o + k]
+        o += k
+        err = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-12)
+        assert err < 2e-2, (name, err)

@@ -14,6 +14,8 @@ import subprocess
 
 import pytest
 
+from tests import fasta
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 GOLD = os.path.join(HERE, "golden")
@@ -28,7 +30,7 @@ pytestmark = pytest.mark.gpu
 def test_reference_main_with_gpu_poa(case):
     if not os.path.exists(BIN):
         pytest.fail("oracle/_ref/minipoa_gpu is missing: build it with `make -C oracle shim REF=<reference tree>`")
-    fa = os.path.join(GOLD, case["case"] + ".fa")
+    fa = fasta.golden_input(case)
     opts = [os.path.join(GOLD, o) if k > 0 and case["opts"][k - 1] == "-i" else o
             for k, o in enumerate(case["opts"])]
     env = dict(os.environ, POA_SHIM_STATS="1")

@@ -73,7 +73,7 @@ def opts_to_params(opts):
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
 def test_model_matches_reference(case, model):
-    names, seqs = fasta.read(os.path.join(GOLD, case["case"] + ".fa"))
+    names, seqs = fasta.read(fasta.golden_input(case))
     n = len(seqs)
     arr = (ctypes.c_char_p * max(n, 1))(*seqs)
     lens = (ctypes.c_int * max(n, 1))(*[len(s) for s in seqs])
@@ -83,7 +83,7 @@ def test_model_matches_reference(case, model):
     if "-i" in case["opts"]:
         with open(os.path.join(GOLD, case["opts"][case["opts"].index("-i") + 1]), "rb") as fh:
             g = fh.read()
-        hdr = fasta.headers(os.path.join(GOLD, case["case"] + ".fa"))
+        hdr = fasta.headers(fasta.golden_input(case))
         harr = (ctypes.c_char_p * max(n, 1))(*[h.encode() for h in hdr])
         st = model.model_run_gfa(n, arr, lens, par, g, len(g), harr, ctypes.byref(out), scores, n + 1)
     else:

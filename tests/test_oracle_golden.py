@@ -11,6 +11,8 @@ import subprocess
 
 import pytest
 
+from tests import fasta
+
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 with open(os.path.join(GOLD, "manifest.json")) as fh:
     MANIFEST = json.load(fh)
@@ -22,7 +24,7 @@ CASES = [c for c in MANIFEST if not {"-S", "-p", "-i"} & set(c["opts"])]
 
 @pytest.mark.parametrize("case", CASES, ids=[c["case"] for c in CASES])
 def test_restatement_matches_reference(case, oracle_bin, tmp_path):
-    fa = os.path.join(GOLD, case["case"] + ".fa")
+    fa = fasta.golden_input(case)
     args = [oracle_bin, fa] + case["opts"]
     dump = tmp_path / "o.dump"
     if case["dump"]:

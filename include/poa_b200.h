@@ -139,6 +139,16 @@ int poa_batch_download(poa_ctx* ctx, char* cons, int64_t cons_cap, int64_t* cons
 int poa_batch_consensus(poa_ctx* ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
                         const int32_t* read_len, int32_t n_reads, const int32_t* win_off, int32_t n_windows,
                         char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status);
+/* The same from files, streamed (no counterpart in the reference beyond its
+ * reader, src/handle_input.cpp:13-43): window w is the FASTA / FASTQ file
+ * paths[w] (plain or gzip), read as one minipoa run reads its input. Files
+ * go in chunks of `chunk` windows; `threads` host threads (0 = all cores)
+ * read and parse chunk k+1 into page-locked memory while chunk k runs on the
+ * device. A chunk should hold several times the resident windows (the
+ * batch's slot count) to keep the device busy. Outputs as poa_batch_consensus for all
+ * n_files windows; a file that cannot be read returns POA_BAD_ARG. */
+int poa_batch_consensus_files(poa_ctx* ctx, const char* const* paths, int32_t n_files, int32_t chunk,
+                              int32_t threads, char* cons, int64_t cons_cap, int64_t* cons_off, int32_t* status);
 /* [0] band cells of the last run, [1] windows that failed, [2] concurrent
  * slots, [3] bytes per slot, [4] H2D bytes of the upload, [5] D2H bytes,
  * [6..11] summed per-window clock cycles of the view build, DP fill,

@@ -146,6 +146,9 @@ def lib() -> ctypes.CDLL:
     L.poa_free_pinned.argtypes = [ctypes.c_void_p]
     L.poa_int_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                ctypes.POINTER(ctypes.c_double)]
+    L.poa_batch_consensus_files.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64, _i64p,
+                                            _i32p]
     L.poa_batch_partition.argtypes = [_i32p, _i32p, ctypes.c_int32, ctypes.c_int32, _i32p, _i64p]
     L.poa_batch_consensus_multi.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int32, _u8p, ctypes.c_int64,
                                             _i64p, _i32p, ctypes.c_int32, _i32p, ctypes.c_int32, ctypes.c_void_p,
@@ -276,6 +279,25 @@ class Context:
         self._nwin = nwin
         raw = cons.raw
         return [raw[off[w]:off[w + 1]] for w in range(nwin)], [int(x) for x in st[:nwin]]
+
+    def batch_consensus_files(self, paths, chunk: int = 20000, threads: int = 0, cons_cap: int = 0):
+        """Windows from FASTA / FASTQ files (one window per file, plain or gzip),
+        parsed on host threads while the device runs the previous chunk
+        (poa_batch_consensus_files). Returns (consensus bytes, status) per file."""
+        import numpy as np
+        n = len(paths)
+        arr = (ctypes.c_char_p * max(n, 1))(*[os.fsencode(p) for p in paths])
+        if cons_cap <= 0:
+            # a consensus is never longer than its window's bases (<= the file, or ~10x a gzip file)
+            cons_cap = sum(os.path.getsize(p) * (10 if str(p).endswith(".gz") else 1) + 64 for p in paths) + 4096
+        cons = ctypes.create_string_buffer(max(cons_cap, 1))
+        off = np.zeros(n + 1, dtype=np.int64)
+        st = np.zeros(max(n, 1), dtype=np.int32)
+        i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        self._check(lib().poa_batch_consensus_files(self._h, arr, n, chunk, threads, cons, cons_cap,
+                                                    off.ctypes.data_as(i64p), st.ctypes.data_as(i32p)))
+        raw = cons.raw
+        return [raw[off[w]:off[w + 1]] for w in range(n)], [int(x) for x in st[:n]]
 
     def batch_read_stats(self):
         """int32 array [n_reads, 8] of the last run: widest row (blocks), cells, rows,

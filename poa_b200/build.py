@@ -23,7 +23,7 @@ CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 CU_SRCS = ["gpu_engine.cu", "batch.cu", "noalloc.cu", "proposer.cu", "intpeak.cu"]
-CPP_SRCS = ["graph.cpp", "driver.cpp", "seeding.cpp", "capi.cpp", "multi.cpp"]
+CPP_SRCS = ["graph.cpp", "driver.cpp", "seeding.cpp", "capi.cpp", "multi.cpp", "stream.cpp", "reader.cpp"]
 HEADERS = [f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] if os.path.isdir(CSRC) else []
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
@@ -69,11 +69,11 @@ def build(verbose: bool = False) -> str:
         objs.append(obj)
     if not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         _run(["g++", "-shared", "-o", LIB] + objs +
-             ["-L" + os.path.join(CUDA, "lib64"), "-lcudart_static", "-ldl", "-lrt", "-lpthread"])
+             ["-L" + os.path.join(CUDA, "lib64"), "-lcudart_static", "-lz", "-ldl", "-lrt", "-lpthread"])
     main = os.path.join(CSRC, "main.cpp")
     if os.path.exists(main) and (not os.path.exists(CLI) or os.path.getmtime(main) > os.path.getmtime(CLI)
                                  or os.path.getmtime(LIB) > os.path.getmtime(CLI)):
-        _run(["g++", "-O2", "-std=c++17", main, "-o", CLI, "-L" + PKG, "-lpoa_b200",
+        _run(["g++", "-O2", "-std=c++17", "-I" + CSRC, main, "-o", CLI, "-L" + PKG, "-lpoa_b200",
               "-Wl,-rpath,$ORIGIN", "-lz"])
     if verbose:
         print("built", LIB)

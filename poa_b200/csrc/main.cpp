@@ -20,58 +20,9 @@
 #include <vector>
 
 #include "../../include/poa_b200.h"
+#include "reader.h"
 
 namespace {
-
-struct Rec {
-    std::string name, comment, seq;
-};
-
-bool read_all(const char* path, std::string& out) {
-    gzFile fp = gzopen(path, "r");
-    if (!fp) return false;
-    char buf[1 << 16];
-    int n;
-    while ((n = gzread(fp, buf, sizeof(buf))) > 0) out.append(buf, (size_t)n);
-    gzclose(fp);
-    return n >= 0;
-}
-
-// FASTA / FASTQ records: name up to the first blank, the rest of the header
-// line is the comment (kseq semantics).
-std::vector<Rec> parse(const std::string& s) {
-    std::vector<Rec> recs;
-    size_t i = 0, n = s.size();
-    while (i < n) {
-        if (s[i] != '>' && s[i] != '@') { i++; continue; }
-        const bool fq = s[i] == '@';
-        size_t eol = s.find('\n', i);
-        if (eol == std::string::npos) eol = n;
-        size_t he = eol;
-        if (he > i + 1 && s[he - 1] == '\r') he--;
-        std::string hdr = s.substr(i + 1, he - i - 1);
-        Rec r;
-        size_t sp = hdr.find_first_of(" \t");
-        r.name = hdr.substr(0, sp);
-        if (sp != std::string::npos) r.comment = hdr.substr(sp + 1);
-        i = eol < n ? eol + 1 : n;
-        while (i < n && s[i] != '>' && !(fq && s[i] == '+') && !(!fq && s[i] == '@')) {
-            if (s[i] != '\n' && s[i] != '\r') r.seq.push_back(s[i]);
-            i++;
-        }
-        if (fq && i < n && s[i] == '+') {
-            size_t e2 = s.find('\n', i);
-            i = e2 == std::string::npos ? n : e2 + 1;
-            size_t ql = 0;
-            while (i < n && ql < r.seq.size()) {
-                if (s[i] != '\n' && s[i] != '\r') ql++;
-                i++;
-            }
-        }
-        recs.push_back(std::move(r));
-    }
-    return recs;
-}
 
 void usage() {
     std::cout << "minipoa_b200 <in.fa> [options]\n"
@@ -153,11 +104,11 @@ int main(int argc, char** argv) {
         if (!done) { std::cerr << "error parsing options: unknown option " << o << "\n"; return 1; }
     }
     std::string data;
-    if (!path.empty() && !read_all(path.c_str(), data)) {
+    if (!path.empty() && !pb::read_file(path.c_str(), data)) {
         std::cerr << "error read file: Error opening file " << path << std::endl;
         return 1;
     }
-    std::vector<Rec> recs = parse(data);
+    std::vector<pb::SeqRec> recs = pb::parse_fastx(data);
     poa_ctx* ctx = poa_create(0, &p);
     if (!ctx) { std::cerr << "no usable CUDA device\n"; return 1; }
     std::vector<const char*> seqs(recs.size()), hdrs(recs.size());
@@ -175,7 +126,7 @@ int main(int argc, char** argv) {
     if (!inc_fp.empty()) {
         // an unreadable graph file leaves the graph empty, as read_gfa does (src/handle_input.cpp:453-455)
         std::string gfa;
-        if (!read_all(inc_fp.c_str(), gfa)) gfa.clear();
+        if (!pb::read_file(inc_fp.c_str(), gfa)) gfa.clear();
         st = poa_run_gfa(ctx, gfa.data(), gfa.size(), (int32_t)recs.size(), seqs.data(), lens.data(), hdrs.data(),
                          &text, &tl, nullptr);
     } else {

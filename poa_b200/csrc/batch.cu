@@ -1303,7 +1303,11 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
                         r[l] = own | (w & W_DEXT) | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
                     }
                 } else {
-                    // every choice by the backtrack's own test, over every predecessor
+                    // the diagonal choices by the backtrack's own test, over every predecessor;
+                    // the vertical choices in z stand (the fill's and the backtrack's vertical
+                    // tests are the same block test) unless the row has more predecessors
+                    // than z's 4-bit positions hold
+                    const bool dwide = d > TRACK_MAX_D;
                     uint32_t cm[BLK], cd[BLK];
 #pragma unroll
                     for (int l = 0; l < BLK; l++) cm[l] = cd[l] = 0x01ff01ffu;
@@ -1316,13 +1320,28 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
                         const uint32_t pos = (uint32_t)ek.z >> 16;
                         const int pbase = ek.w & 255;
                         const uint32_t m1v = (ek.w & 256) ? pos : 510u;
-                        int32_t Mb[BLK], Db[BLK];
+                        int32_t Mb[BLK];
                         int32_t mprev = NEG_INF;
                         if (mk.prev_in) mprev = src[(B - 1 - pBs) * 16 + 7];
-                        if (mk.blk_in) load_block16(src + (B - pBs) * 16, Mb, Db);
-                        else {
+                        if (mk.blk_in) {
+                            const int4* q = reinterpret_cast<const int4*>(src + (B - pBs) * 16);
+                            const int4 u = q[0], v = q[1];
+                            Mb[0] = u.x; Mb[1] = u.y; Mb[2] = u.z; Mb[3] = u.w;
+                            Mb[4] = v.x; Mb[5] = v.y; Mb[6] = v.z; Mb[7] = v.w;
+                            if (dwide) {
+                                const int4 x = q[2], y = q[3];
+                                const int32_t Db[BLK] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
 #pragma unroll
-                            for (int l = 0; l < BLK; l++) Mb[l] = Db[l] = NEG_INF;
+                                for (int l = 0; l < BLK; l++) {
+                                    if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
+                                        cd[l] = (cd[l] & 0xffff0000u) | pos;
+                                    if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
+                                        cd[l] = (cd[l] & 0xffffu) | (pos << 16);
+                                }
+                            }
+                        } else {
+#pragma unroll
+                            for (int l = 0; l < BLK; l++) Mb[l] = NEG_INF;
                         }
 #pragma unroll
                         for (int l = 0; l < BLK; l++) {
@@ -1332,26 +1351,26 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
                             const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
                             if (eqM && (cm[l] >> 16) == 511u) cm[l] = (cm[l] & 0xffffu) | (pos << 16);
                             if (eqM && bm && (cm[l] & 0xffffu) == 511u) cm[l] = (cm[l] & 0xffff0000u) | m1v;
-                            if (mk.blk_in) {
-                                if ((cd[l] & 0xffffu) == 511u && Dv[l] == add32(Mb[l], sc.o1))
-                                    cd[l] = (cd[l] & 0xffff0000u) | pos;
-                                if ((cd[l] >> 16) == 511u && Dv[l] == add32(Db[l], sc.e1))
-                                    cd[l] = (cd[l] & 0xffffu) | (pos << 16);
-                            }
                         }
                     }
 #pragma unroll
                     for (int l = 0; l < BLK; l++) {
                         const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                        uint32_t w = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
-                        uint32_t m1 = cm[l] & 0xffffu, m4 = cm[l] >> 16;
+                        const uint32_t own = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il) & 15u;
+                        const uint32_t w = (z2[l >> 1] >> (16 * (l & 1))) & 0xffffu;
+                        uint32_t m1 = cm[l] & 0xffffu;
                         if (m1 == 510u) m1 = W_NONE;
-                        uint32_t dd = cd[l] & 0xffffu;
-                        if (dd == 511u) {
-                            dd = cd[l] >> 16;
-                            if (dd != 511u) w |= W_DEXT;
+                        const uint32_t m4 = cm[l] >> 16, nd = w & 15u;
+                        uint32_t dd = nd != Y_NONE ? nd : W_NONE, dext = w & W_DEXT;
+                        if (dwide) {
+                            dd = cd[l] & 0xffffu;
+                            dext = 0;
+                            if (dd == 511u) {
+                                dd = cd[l] >> 16;
+                                if (dd != 511u) dext = W_DEXT;
+                            }
                         }
-                        r[l] = w | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
+                        r[l] = own | dext | (m1 << W_M1_SHIFT) | (m4 << W_M4_SHIFT) | (dd << W_D_SHIFT);
                     }
                 }
                 uint4* tdst = reinterpret_cast<uint4*>(a.tb + cur.tb + b * BLK * 4);

@@ -197,3 +197,34 @@ def test_streamed_files_match_reference(tmp_path):
     for (nm, _), c, s in zip(paths, cons, status):
         with open(os.path.join(GOLD, nm + ".out"), "rb") as fh:
             assert s == 0 and b">consensus sequence\n" + c + b"\n" == fh.read(), nm
+
+
+def _many_pred_window(seed):
+    """Reads that delete 1..23 bases before one template position, substitute its
+    left neighbour or insert a base before it: that node gets 22 in-window
+    predecessors (seed 61), beyond the 15 the fill's one-pass record choices
+    hold, so its row takes the full second pass."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = synth.to_ascii(synth.random_root(rng, 320))
+    P = 200
+    sub = [t[:P - 1] + bytes([b]) + t[P:] for b in b"ACGT" if b != t[P - 1]]
+    ins = [t[:P] + bytes([b]) + t[P:] for b in b"ACGT"]
+    return [t] + [t[:P - k] + t[P:] for k in range(1, 24)] + sub + ins  # one node with 22 predecessors
+
+
+@pytest.mark.parametrize("opts", [[], ["-B"]])
+def test_batch_rows_with_many_predecessors(opts, oracle_bin, tmp_path):
+    wins = [_many_pred_window(s) for s in (61, 62)]
+    reads, offs = [], [0]
+    for rs in wins:
+        reads.extend(rs)
+        offs.append(offs[-1] + len(rs))
+    ws = synth.pack_windows_from_reads(reads, offs)
+    with poa_b200.Context(poa_b200.Params.from_cli(opts)) as ctx:
+        cons, st = ctx.batch_consensus(ws)
+    for w, rs in enumerate(wins):
+        fa = tmp_path / f"w{w}.fa"
+        synth.write_fasta(str(fa), rs)
+        want = _cons_of(subprocess.run([oracle_bin, str(fa)] + opts, capture_output=True, check=True).stdout)
+        assert st[w] == 0 and cons[w] == want

@@ -1128,6 +1128,7 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
         uint32_t z2[BLK / 2];  // choice words: cell 2t in bits 0..15, cell 2t+1 in bits 16..31
         int32_t cmprev = NEG_INF;
         bool c_blk = false, c_prev = false, slow = d > TRACK_MAX_D, slow0 = false;
+        uint32_t f1lo = 0, f1hi = 0, m1lo = 0, m1hi = 0;  // one predecessor: record flags, see below
         uint32_t hm = 0;  // bit l: Mpre[l] >= Dv[l], then (after the scan) M[l] == Mpre[l]
         uint32_t qlo = 0x04040404u, qhi = 0x04040404u;
         const int32_t minit = multi ? INT_MIN : NEG_INF;
@@ -1175,12 +1176,36 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
                             }
                         }
                     } else {
-                        uint8_t qc8[BLK];
+                        // one predecessor: its terms and, while they are in registers, the
+                        // 1-byte record's predecessor flags (byte l of f1lo / f1hi): the
+                        // vertical choice (the fill's and the backtrack's vertical tests are
+                        // the same block test) and the diagonal one, which stands when
+                        // M == Mpre (checked after the scan) wherever the fill's diagonal
+                        // mask matches the backtrack's per-cell test (else slow: recomputed)
 #pragma unroll
-                        for (int l = 0; l < BLK; l++) qc8[l] = (uint8_t)qc_at(l);
-                        pass1_pred(sc, mk, b == 0, pbase, Mb, Db, mprev, qc8, Mpre, Dv);
+                        for (int l = 0; l < BLK; l++) {
+                            const int32_t ce = add32(Db[l], sc.e1), co = add32(Mb[l], sc.o1);
+                            const int32_t dv = mx(mx(NEG_INF, ce), co);
+                            Dv[l] = dv;
+                            const uint32_t fd = co == dv ? R_DOPEN : (ce == dv ? R_DEXT : 0u);
+                            if (l < 4) f1lo |= fd << (8 * l);
+                            else f1hi |= fd << (8 * (l - 4));
+                        }
+                        if (mk.diag) {
 #pragma unroll
-                        for (int l = 0; l < BLK; l++) { pa[l] = Mb[l]; pb[l] = Db[l]; }
+                            for (int l = 0; l < BLK; l++) {
+                                const bool bm = pbase == qc_at(l);
+                                const int32_t src0 = l == 0 ? (b == 0 ? NEG_INF : mprev) : Mb[l > 0 ? l - 1 : 0];
+                                const int32_t cand = add32(src0, bm ? sc.match : sc.mismatch);
+                                const int32_t mp = mx(NEG_INF, cand);
+                                Mpre[l] = mp;
+                                // cell 0 counts only where the backtrack tests the same value
+                                const bool tested = l > 0 || (mk.prev_in && b != 0);
+                                const uint32_t fm = (tested && cand == mp) ? (R_M4 | ((bm && cur.w1ok) ? R_M1 : 0u)) : 0u;
+                                if (l < 4) m1lo |= fm << (8 * l);
+                                else m1hi |= fm << (8 * (l - 4));
+                            }
+                        }
                     }
                 }
                 if (multi) {
@@ -1188,6 +1213,7 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
                     slow0 |= mk.prev_in && !(mk.blk_in && mk.diag && b != 0);
                 } else {
                     cmprev = mprev; c_blk = mk.blk_in; c_prev = mk.prev_in;
+                    slow |= (mk.blk_in && !mk.diag) || (mk.prev_in && !(mk.blk_in && mk.diag && b != 0));
                 }
             }
         }
@@ -1251,19 +1277,43 @@ __device__ __forceinline__ void fill_row_dyn(const DpArgs& a, const RowDesc& cur
 #pragma unroll
                 for (int l = 0; l < BLK; l++) {
                     const int32_t Ml = l > 0 ? M[l - 1] : Ml0, Il = l > 0 ? I[l - 1] : Il0;
-                    uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
-                    if (d == 1) {
-                        const bool inr = l == 0 ? c_prev : c_blk;
-                        const int32_t mv = l == 0 ? cmprev : pa[l > 0 ? l - 1 : 0];
-                        const bool bm = cur.pbase == qc_at(l);
-                        const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
-                        if (eqM) r |= R_M4;
-                        if (eqM && bm && cur.w1ok) r |= R_M1;
-                        if (c_blk && Dv[l] == add32(pa[l], sc.o1)) r |= R_DOPEN;
-                        else if (c_blk && Dv[l] == add32(pb[l], sc.e1)) r |= R_DEXT;
-                    }
+                    const uint32_t r = own_flags(sc, j0 + l, M[l], Dv[l], I[l], Ml, Il);
                     if (l < 4) lo |= r << (8 * l);
                     else hi |= r << (8 * (l - 4));
+                }
+                if (d == 1) {
+                    // the diagonal flags stand in cells where M == Mpre (byte mask of hm)
+                    const uint32_t hlo = ((hm & 15u) * 0x00204081u & 0x01010101u) * 0xffu;
+                    const uint32_t hhi = ((hm >> 4) * 0x00204081u & 0x01010101u) * 0xffu;
+                    lo |= f1lo | (m1lo & hlo);
+                    hi |= f1hi | (m1hi & hhi);
+                    if (slow) {
+                        // a block where the fill's diagonal mask and the backtrack's per-cell
+                        // test differ: the diagonal flags by the backtrack's own test
+                        const int pBs = cur.pbsbe & 0xffff;
+                        const int32_t* src = a.rs + cur.pst;
+                        int32_t Mb[BLK];
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) Mb[l] = NEG_INF;
+                        if (c_blk) {
+                            const int4* q = reinterpret_cast<const int4*>(src + (B - pBs) * 16);
+                            const int4 u = q[0], v = q[1];
+                            Mb[0] = u.x; Mb[1] = u.y; Mb[2] = u.z; Mb[3] = u.w;
+                            Mb[4] = v.x; Mb[5] = v.y; Mb[6] = v.z; Mb[7] = v.w;
+                        }
+                        lo &= ~0x30303030u;
+                        hi &= ~0x30303030u;
+#pragma unroll
+                        for (int l = 0; l < BLK; l++) {
+                            const bool inr = l == 0 ? c_prev : c_blk;
+                            const int32_t mv = l == 0 ? cmprev : Mb[l > 0 ? l - 1 : 0];
+                            const bool bm = cur.pbase == qc_at(l);
+                            const bool eqM = inr && M[l] == add32(mv, bm ? sc.match : sc.mismatch);
+                            const uint32_t fm = eqM ? (R_M4 | ((bm && cur.w1ok) ? R_M1 : 0u)) : 0u;
+                            if (l < 4) lo |= fm << (8 * l);
+                            else hi |= fm << (8 * (l - 4));
+                        }
+                    }
                 }
                 *reinterpret_cast<uint2*>(a.tb + cur.tb + b * BLK) = make_uint2(lo, hi);
             } else {

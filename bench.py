@@ -414,6 +414,27 @@ def ours(args, world, rank, local, D):
     cells = st["cells"]
     failed = int(D.sum(st["failed"]))
     cons, status = ctx.batch_download()
+    plan_check = None
+    if prop is not None:
+        # how often a window's real need exceeded its OWN predicted need (nodes, record
+        # bytes of its largest alignment, spilled entries), apart from the launch's slot
+        # sizing (every slot sized for the largest predicted window, x PLAN_HEADROOM)
+        import numpy as np
+        p_nodes, p_tb, p_sp = ctx.batch_plan_get()
+        rs = ctx.batch_read_stats()
+        woff = ws.win_off
+        miss = 0
+        for w in range(ws.n_windows):
+            a, b = int(woff[w]), int(woff[w + 1])
+            if b <= a:
+                continue
+            r = rs[a:b]
+            if r[-1, 3] > p_nodes[w] or r[:, 4].max() > p_tb[w] or r[:, 5].max() > p_sp[w]:
+                miss += 1
+        plan_check = {"windows_over_own_prediction": miss, "rate": miss / max(ws.n_windows, 1),
+                      "slot_headroom": 1.5,
+                      "note": "slots are sized for the largest predicted window x 1.5 (memory allowing); "
+                              "this counts windows whose need exceeded their own prediction"}
     # every window of the whole set against the reference's per-window manifest
     all_cons = cons if world == 1 else gather_in_order(D, mine, cons, full.n_windows)
     parity_full = manifest_check(wl, all_cons) if (rank == 0 and not args.reads_per_window) else None
@@ -500,7 +521,8 @@ def ours(args, world, rank, local, D):
                             "fallback_rate": D.sum(fallback) / (world * ws.n_windows * args.steps),
                             "plan_ms_per_step": sum(plan_ms) / args.steps,
                             "weights": os.path.relpath(poa_b200.PROP_WEIGHTS, ROOT),
-                            "exact": "the plan sizes slots only; every DP runs the reference band"}
+                            "exact": "the plan sizes slots only; every DP runs the reference band",
+                            "per_window": plan_check}
     if rank == 0 and world == 1 and args.plain_windows > 0:
         # the plain single-alignment kernel on the first windows of the same set
         n = min(args.plain_windows, ws.n_windows)

@@ -172,6 +172,12 @@ int poa_batch_stats(poa_ctx* ctx, int64_t* out19);
  * the plan; poa_batch_upload clears it too. */
 int poa_batch_plan(poa_ctx* ctx, const int32_t* nodes, const int64_t* tb_bytes, const int64_t* spill,
                    const float* cost);
+/* The per-window plan the last run used (set by poa_batch_plan or the
+ * proposer): graph nodes, record bytes of the largest alignment and spilled
+ * row-store entries, n_windows values each. With poa_batch_read_stats it
+ * shows how often a window's real need exceeded its own prediction, apart
+ * from the slot headroom that the launch adds. */
+int poa_batch_plan_get(poa_ctx* ctx, int32_t* nodes, int64_t* tb_bytes, int64_t* spill, int32_t n_windows);
 /* Per read of the last run, 8 values each (n_reads * 8 entries): widest DP
  * row in 8-column blocks, band cells, DP rows, graph nodes after fusing the
  * read, traceback record bytes, spilled row-store entries (int32), graph

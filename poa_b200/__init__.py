@@ -126,6 +126,7 @@ def lib() -> ctypes.CDLL:
     L.poa_batch_config.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
     L.poa_batch_read_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64]
     L.poa_batch_plan.argtypes = [ctypes.c_void_p] * 5
+    L.poa_batch_plan_get.argtypes = [ctypes.c_void_p, _i32p, _i64p, _i64p, ctypes.c_int32]
     L.poa_prop_create.restype = ctypes.c_void_p
     L.poa_prop_create.argtypes = [ctypes.c_int]
     L.poa_prop_destroy.argtypes = [ctypes.c_void_p]
@@ -307,6 +308,18 @@ class Context:
         out = np.zeros((max(n, 1), 8), dtype=np.int32)
         self._check(lib().poa_batch_read_stats(self._h, out.ctypes.data, out.size))
         return out[:n]
+
+    def batch_plan_get(self):
+        """(nodes, record bytes, spilled entries) per window of the last planned run."""
+        import numpy as np
+        n = int(self._nwin)
+        nodes = np.zeros(max(n, 1), dtype=np.int32)
+        tb = np.zeros(max(n, 1), dtype=np.int64)
+        sp = np.zeros(max(n, 1), dtype=np.int64)
+        i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+        self._check(lib().poa_batch_plan_get(self._h, nodes.ctypes.data_as(i32p), tb.ctypes.data_as(i64p),
+                                             sp.ctypes.data_as(i64p), n))
+        return nodes[:n], tb[:n], sp[:n]
 
     def batch_features(self, prop: "Proposer"):
         """float32 [n_reads, 32, 8] proposer features of the uploaded windows."""

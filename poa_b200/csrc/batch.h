@@ -113,6 +113,13 @@ class BatchEngine {
     void* evr0_ = nullptr;
     void* evr1_ = nullptr;
     void* evp_ = nullptr;
+  public:
+    // the plan of the last planned run (empty when the run had none)
+    const std::vector<int32_t>& plan_nodes() const { return plan_nodes_; }
+    const std::vector<int64_t>& plan_tb() const { return plan_tb_; }
+    const std::vector<int64_t>& plan_spill() const { return plan_spill_; }
+
+  private:
     std::vector<int32_t> plan_nodes_, plan_order_;
     std::vector<int64_t> plan_tb_, plan_spill_;
     int device_;

@@ -355,6 +355,19 @@ int poa_batch_plan(poa_ctx* ctx, const int32_t* nodes, const int64_t* tb_bytes, 
     return POA_OK;
 }
 
+int poa_batch_plan_get(poa_ctx* ctx, int32_t* nodes, int64_t* tb_bytes, int64_t* spill, int32_t n_windows) {
+    if (!ctx || !ctx->batch || !nodes || !tb_bytes || !spill) return fail(ctx, POA_BAD_ARG, "null argument");
+    const pb::BatchEngine& b = *ctx->batch;
+    if (b.plan_nodes().empty()) return fail(ctx, POA_BAD_ARG, "the last run had no plan");
+    if ((size_t)n_windows != b.plan_nodes().size()) return fail(ctx, POA_BAD_ARG, "window count differs from the plan");
+    for (int32_t w = 0; w < n_windows; w++) {
+        nodes[w] = b.plan_nodes()[w];
+        tb_bytes[w] = b.plan_tb()[w];
+        spill[w] = b.plan_spill()[w];
+    }
+    return POA_OK;
+}
+
 int poa_batch_config(poa_ctx* ctx, int32_t key, int64_t value) {
     if (!ctx) return POA_BAD_ARG;
     try {

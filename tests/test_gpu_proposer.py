@@ -81,6 +81,9 @@ def test_planned_run_is_exact_and_smaller():
         ctx.batch_run()
         cons1, st1 = ctx.batch_download()
         s1 = ctx.batch_stats()
+        # the per-window plan the run used, against each window's real need
+        p_nodes, p_tb, p_sp = ctx.batch_plan_get()
+        rs = ctx.batch_read_stats()
         # the same through the host-buffer entry point
         cons2, st2 = ctx.batch_consensus(ws)
     assert st0 == [0] * ws.n_windows
@@ -90,6 +93,12 @@ def test_planned_run_is_exact_and_smaller():
     assert s1["plan_us"] > 0 and s1["run_us"] >= s1["kernel_us"]
     assert s1["fallback"] <= 1
     assert s1["slot_bytes"] < s0["slot_bytes"]
+    assert p_nodes.shape == (ws.n_windows,) and (p_nodes > 2).all() and (p_tb > 0).all()
+    over = 0
+    for w in range(ws.n_windows):
+        a, b = int(ws.win_off[w]), int(ws.win_off[w + 1])
+        over += int(rs[b - 1, 3] > p_nodes[w] or rs[a:b, 4].max() > p_tb[w])
+    assert over <= max(1, ws.n_windows // 10)  # each window's own prediction mostly covers it
 
 
 def test_undersized_plan_falls_back_exactly():

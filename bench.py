@@ -620,7 +620,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="learned_band")
     ap.add_argument("--windows", type=int, default=0, help="windows per rank (default: the workload's)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--plain-windows", type=int, default=2,
+    ap.add_argument("--plain-windows", type=int, default=8,
                     help="windows timed on the plain single-alignment kernel path (0 = skip)")
     ap.add_argument("--e2e-warmup", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")

@@ -82,7 +82,6 @@ def log(*a):
 def rank_windows(ws, world: int, rank: int):
     """This rank's share of one window set: the cost-balanced split of
     poa_batch_partition (longest processing time first), in input order."""
-    import numpy as np
     if world == 1:
         return np.arange(ws.n_windows)
     import poa_b200
@@ -419,7 +418,6 @@ def ours(args, world, rank, local, D):
         # how often a window's real need exceeded its OWN predicted need (nodes, record
         # bytes of its largest alignment, spilled entries), apart from the launch's slot
         # sizing (every slot sized for the largest predicted window, x PLAN_HEADROOM)
-        import numpy as np
         p_nodes, p_tb, p_sp = ctx.batch_plan_get()
         rs = ctx.batch_read_stats()
         woff = ws.win_off

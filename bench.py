@@ -343,7 +343,7 @@ def manifest_check(wl, cons):
     with open(p) as fh:
         head = json.loads(fh.readline()[2:])
         want = [ln.strip() for ln in fh]
-    if head["kwargs"]["seed"] != wl["seed"] or len(cons) < head["windows"]:
+    if head["kwargs"]["seed"] != wl["seed"] or len(cons) != head["windows"]:
         return None  # another set (the chimeric reads depend on the set's size)
     n = min(len(want), len(cons))
     same = sum(1 for w in range(n) if hashlib.md5(cons[w]).hexdigest()[:16] == want[w])

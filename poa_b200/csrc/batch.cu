@@ -1822,13 +1822,35 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, unsigned 
     const bool lens = A.f > 0;
     constexpr bool static_band = STATIC;  // f > 0 && !ab_band (checked on the host)
     int status = ST_OK;
-    int64_t cells = 0, ecells = 0;
-    long long ph[NPHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // the window's counters: in registers for the adaptive-band kernel; in the
+    // window's output slots (lane 0) for the static-band kernel, whose fill
+    // runs faster with the registers free (measured)
+    int64_t cells_r = 0, ecells_r = 0;
+    long long ph_r[NPHASE] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t* const cells_g = A.cells + 2 * (int64_t)w;
+    int64_t* const ph_g = A.phase + (int64_t)w * NPHASE;
+    if (STATIC && lane == 0) {
+        cells_g[0] = cells_g[1] = 0;
+        for (int k = 0; k < NPHASE; k++) ph_g[k] = 0;
+    }
     long long tc = clock64();
     auto tick = [&](int k) {
         long long t = clock64();
-        ph[k] += t - tc;
+        if constexpr (STATIC) {
+            if (lane == 0) ph_g[k] += t - tc;
+        } else {
+            ph_r[k] += t - tc;
+        }
         tc = t;
+    };
+    auto add_cells = [&](int64_t c, int64_t e) {  // lane 0
+        if constexpr (STATIC) {
+            cells_g[0] += c;
+            cells_g[1] += e;
+        } else {
+            cells_r += c;
+            ecells_r += e;
+        }
     };
     for (int x = lane; x < L.NC; x += 32) { g.hlen[x] = 0; g.tlen[x] = 0; }
     if (lane == 0) {
@@ -1961,16 +1983,14 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, unsigned 
                 st = bt_warp_static((const RowDesc*)(s + L.v_desc), a.v.in_row, a.v.in_base, a.tb, qs, v.n, len + 1,
                                     a.moves, a.moves_cap, nm, lane);
             if (lane == 0) {
-                cells += a.out[3];
-                ecells += a.out[6];
+                add_cells(a.out[3], a.out[6]);
                 g.hdr[2] = st;
                 g.hdr[13] = nm;
                 g.hdr[12] = g.hdr[12] + 1;  // fusion stamp, increasing over the slot's lifetime
             }
         } else if (lane == 0) {
             int st = a.out[0];
-            cells += a.out[3];
-            ecells += a.out[6];
+            add_cells(a.out[3], a.out[6]);
             int32_t nm = 0;
             if (st == ST_OK) st = backtrack_records(a, len + 1, nm);
             g.hdr[2] = st;
@@ -2013,9 +2033,11 @@ __device__ void process_window(const BatchArgs& A, char* s, DpArgs& a, unsigned 
         tick(PH_CONS);
         A.cons_len[w] = len < 0 ? 0 : len;
         A.status[w] = status;
-        A.cells[2 * (int64_t)w] = cells;
-        A.cells[2 * (int64_t)w + 1] = ecells;
-        for (int k = 0; k < NPHASE; k++) A.phase[(int64_t)w * NPHASE + k] = ph[k];
+        if constexpr (!STATIC) {
+            cells_g[0] = cells_r;
+            cells_g[1] = ecells_r;
+            for (int k = 0; k < NPHASE; k++) ph_g[k] = ph_r[k];
+        }
     }
     __syncwarp();
 }

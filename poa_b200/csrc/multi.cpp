@@ -33,7 +33,7 @@ int64_t window_cost(const int32_t* read_len, const int32_t* win_off, int32_t w) 
 
 extern "C" int poa_batch_partition(const int32_t* read_len, const int32_t* win_off, int32_t n_windows,
                                    int32_t n_parts, int32_t* part, int64_t* part_cost) {
-    if (!read_len || !win_off || !part || n_windows < 0 || n_parts < 1) return POA_BAD_ARG;
+    if (!read_len || !win_off || !part || n_windows < 0 || n_parts < 1 || win_off[0] < 0) return POA_BAD_ARG;
     std::vector<int64_t> cost(n_windows);
     for (int32_t w = 0; w < n_windows; w++) {
         if (win_off[w + 1] < win_off[w]) return POA_BAD_ARG;
@@ -55,13 +55,34 @@ extern "C" int poa_batch_partition(const int32_t* read_len, const int32_t* win_o
     return POA_OK;
 }
 
+namespace {
+
+int consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                    const int32_t* read_len, const int32_t* win_off, int32_t n_windows, char* cons,
+                    int64_t cons_cap, int64_t* cons_off, int32_t* status);
+
+}  // namespace
+
 extern "C" int poa_batch_consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const uint8_t* seq, int64_t seq_bytes,
                                          const int64_t* read_off, const int32_t* read_len, int32_t n_reads,
                                          const int32_t* win_off, int32_t n_windows, char* cons, int64_t cons_cap,
                                          int64_t* cons_off, int32_t* status) {
     if (!ctxs || n_ctx < 1 || !read_off || !read_len || !win_off || !cons_off || !status || n_windows < 0 ||
-        n_reads < 0 || win_off[n_windows] > n_reads)
+        n_reads < 0 || win_off[0] < 0 || win_off[n_windows] > n_reads || (cons_cap > 0 && !cons))
         return POA_BAD_ARG;
+    try {
+        return consensus_multi(ctxs, n_ctx, seq, seq_bytes, read_off, read_len, win_off, n_windows, cons, cons_cap,
+                               cons_off, status);
+    } catch (const std::exception&) {
+        return POA_OOM;  // host memory or threads for the split ran out
+    }
+}
+
+namespace {
+
+int consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const uint8_t* seq, int64_t seq_bytes, const int64_t* read_off,
+                    const int32_t* read_len, const int32_t* win_off, int32_t n_windows, char* cons,
+                    int64_t cons_cap, int64_t* cons_off, int32_t* status) {
     for (int32_t g = 0; g < n_ctx; g++)
         if (!ctxs[g]) return POA_BAD_ARG;
     std::vector<int32_t> part(n_windows);
@@ -88,14 +109,25 @@ extern "C" int poa_batch_consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const ui
     for (int32_t g = 0; g < n_ctx; g++) {
         Part& p = parts[g];
         if (p.wins.empty()) continue;
-        threads.emplace_back([&p, g, ctxs, seq, seq_bytes, cons_cap]() {
-            p.cons.resize((size_t)std::max<int64_t>(cons_cap, 1));
-            p.cons_off.resize(p.wins.size() + 1);
-            p.status.resize(p.wins.size());
+        p.rc = POA_OOM;  // until its thread has run
+        auto job = [&p, g, ctxs, seq, seq_bytes, cons_cap]() {
+            try {
+                p.cons.resize((size_t)std::max<int64_t>(cons_cap, 1));
+                p.cons_off.resize(p.wins.size() + 1);
+                p.status.resize(p.wins.size());
+            } catch (const std::exception&) {
+                p.rc = POA_OOM;
+                return;
+            }
             p.rc = poa_batch_consensus(ctxs[g], seq, seq_bytes, p.read_off.data(), p.read_len.data(),
                                        (int32_t)p.read_len.size(), p.win_off.data(), (int32_t)p.wins.size(),
                                        p.cons.data(), (int64_t)p.cons.size(), p.cons_off.data(), p.status.data());
-        });
+        };
+        try {
+            threads.emplace_back(job);
+        } catch (const std::exception&) {
+            job();  // no thread left: this part runs on the calling thread
+        }
     }
     for (auto& t : threads) t.join();
     for (const Part& p : parts)
@@ -118,3 +150,5 @@ extern "C" int poa_batch_consensus_multi(poa_ctx** ctxs, int32_t n_ctx, const ui
     cons_off[n_windows] = pos;
     return POA_OK;
 }
+
+}  // namespace

@@ -12,6 +12,7 @@
 // windows (slots), or the persistent launch runs short of work at its end.
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cstdint>
 #include <cstring>
 #include <future>
@@ -36,30 +37,46 @@ struct Chunk {
     }
 };
 
-void parse_chunk(const char* const* paths, int32_t w0, int32_t w1, int threads, Chunk& c) {
+void parse_chunk_body(const char* const* paths, int32_t w0, int32_t w1, int threads, Chunk& c) {
     const int32_t nw = w1 - w0;
     std::vector<std::vector<pb::SeqRec>> recs(nw);
     std::vector<char> ok(nw, 1);
     std::atomic<int32_t> next(0);
+    std::atomic<bool> oom(false);
     auto work = [&]() {
-        std::string text;
-        for (int32_t k = next++; k < nw; k = next++) {
-            text.clear();
-            if (!pb::read_file(paths[w0 + k], text)) { ok[k] = 0; continue; }
-            recs[k] = pb::parse_fastx(text);
+        try {
+            std::string text;
+            for (int32_t k = next++; k < nw; k = next++) {
+                text.clear();
+                if (!pb::read_file(paths[w0 + k], text)) { ok[k] = 0; continue; }
+                recs[k] = pb::parse_fastx(text);
+            }
+        } catch (const std::exception&) {
+            oom = true;
+            next = nw;  // the other threads stop too
         }
     };
     std::vector<std::thread> pool;
-    for (int t = 1; t < threads; t++) pool.emplace_back(work);
+    for (int t = 1; t < threads; t++) {
+        try {
+            pool.emplace_back(work);
+        } catch (const std::exception&) {
+            break;  // fewer host threads; the calling thread still parses
+        }
+    }
     work();
     for (auto& t : pool) t.join();
+    if (oom) { c.rc = POA_OOM; return; }
     c.read_off.clear();
     c.read_len.clear();
     c.win_off.assign(1, 0);
     int64_t bytes = 0;
     for (int32_t k = 0; k < nw; k++) {
         if (!ok[k]) { c.rc = POA_BAD_ARG; return; }
-        for (const pb::SeqRec& r : recs[k]) bytes += (int64_t)r.seq.size();
+        for (const pb::SeqRec& r : recs[k]) {
+            if (r.seq.size() > (size_t)INT32_MAX) { c.rc = POA_BAD_ARG; return; }
+            bytes += (int64_t)r.seq.size();
+        }
     }
     if (bytes + 16 > c.cap) {
         if (c.seq) poa_free_pinned(c.seq);
@@ -79,6 +96,17 @@ void parse_chunk(const char* const* paths, int32_t w0, int32_t w1, int threads, 
     }
     c.bytes = pos;
     c.rc = POA_OK;
+}
+
+// A chunk that could not be built (host memory, an unreadable file) carries
+// its status in rc; nothing escapes to the caller's thread as an exception.
+void parse_chunk(const char* const* paths, int32_t w0, int32_t w1, int threads, Chunk& c) {
+    c.rc = POA_OK;
+    try {
+        parse_chunk_body(paths, w0, w1, threads, c);
+    } catch (const std::exception&) {
+        c.rc = POA_OOM;
+    }
 }
 
 }  // namespace
@@ -103,9 +131,14 @@ extern "C" int poa_batch_consensus_files(poa_ctx* ctx, const char* const* paths,
         const int32_t w1 = std::min(n_files, w0 + chunk);
         // the next chunk is read and parsed while this one is on the device
         std::future<void> next;
-        if (w1 < n_files)
-            next = std::async(std::launch::async, parse_chunk, paths, w1, std::min(n_files, w1 + chunk), threads,
-                              std::ref(bufs[k ^ 1]));
+        if (w1 < n_files) {
+            try {
+                next = std::async(std::launch::async, parse_chunk, paths, w1, std::min(n_files, w1 + chunk),
+                                  threads, std::ref(bufs[k ^ 1]));
+            } catch (const std::exception&) {
+                parse_chunk(paths, w1, std::min(n_files, w1 + chunk), threads, bufs[k ^ 1]);  // no thread: now
+            }
+        }
         const int32_t nw = w1 - w0;
         int rc = poa_batch_upload(ctx, cur.seq, cur.bytes, cur.read_off.data(), cur.read_len.data(),
                                   (int32_t)cur.read_len.size(), cur.win_off.data(), nw);

@@ -5,6 +5,8 @@ the split must give every window to exactly one part, balance the parts'
 estimated cost (bases x (reads + 1)), follow the longest-processing-time
 rule deterministically, and let the results be put back in input order.
 """
+import types
+
 import numpy as np
 import pytest
 
@@ -62,3 +64,11 @@ def test_empty_and_bad_arguments():
     assert part.shape == (0,) and load.tolist() == [0, 0, 0, 0]
     with pytest.raises(poa_b200.PoaError):
         poa_b200.partition(ws, 0)
+    # offsets that start before the read list, or run backwards, are rejected
+    bad = types.SimpleNamespace(read_len=np.array([5, 5], dtype=np.int32),
+                                win_off=np.array([-1, 2], dtype=np.int32))
+    with pytest.raises(poa_b200.PoaError):
+        poa_b200.partition(bad, 2)
+    bad.win_off = np.array([0, 2, 1], dtype=np.int32)
+    with pytest.raises(poa_b200.PoaError):
+        poa_b200.partition(bad, 2)

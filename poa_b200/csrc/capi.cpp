@@ -258,7 +258,12 @@ int poa_run(poa_ctx* ctx, int32_t nseq, const char* const* seqs, const int32_t* 
 int poa_run_gfa(poa_ctx* ctx, const char* gfa, size_t gfa_len, int32_t nseq, const char* const* seqs,
                 const int32_t* lens, const char* const* headers, char** text, size_t* text_len, int32_t* scores) {
     if (!gfa && gfa_len > 0) return fail(ctx, POA_BAD_ARG, "null GFA text");
-    const std::string g(gfa ? gfa : "", gfa_len);
+    std::string g;
+    try {
+        g.assign(gfa ? gfa : "", gfa_len);
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_OOM, e.what());
+    }
     return run_impl(ctx, &g, nseq, seqs, lens, headers, text, text_len, scores);
 }
 
@@ -351,7 +356,11 @@ int poa_batch_plan(poa_ctx* ctx, const int32_t* nodes, const int64_t* tb_bytes, 
                    const float* cost) {
     if (!ctx || !ctx->batch) return fail(ctx, POA_BAD_ARG, "no uploaded batch");
     if (nodes && (!tb_bytes || !spill || !cost)) return fail(ctx, POA_BAD_ARG, "incomplete plan");
-    ctx->batch->set_plan(nodes, tb_bytes, spill, cost);
+    try {
+        ctx->batch->set_plan(nodes, tb_bytes, spill, cost);
+    } catch (const std::exception& e) {
+        return fail(ctx, POA_OOM, e.what());
+    }
     return POA_OK;
 }
 

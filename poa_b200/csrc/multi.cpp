@@ -29,11 +29,25 @@ int64_t window_cost(const int32_t* read_len, const int32_t* win_off, int32_t w) 
     return bases * (int64_t)(win_off[w + 1] - win_off[w] + 1);
 }
 
+int partition(const int32_t* read_len, const int32_t* win_off, int32_t n_windows, int32_t n_parts, int32_t* part,
+              int64_t* part_cost);
+
 }  // namespace
 
 extern "C" int poa_batch_partition(const int32_t* read_len, const int32_t* win_off, int32_t n_windows,
                                    int32_t n_parts, int32_t* part, int64_t* part_cost) {
     if (!read_len || !win_off || !part || n_windows < 0 || n_parts < 1 || win_off[0] < 0) return POA_BAD_ARG;
+    try {
+        return partition(read_len, win_off, n_windows, n_parts, part, part_cost);
+    } catch (const std::exception&) {
+        return POA_OOM;
+    }
+}
+
+namespace {
+
+int partition(const int32_t* read_len, const int32_t* win_off, int32_t n_windows, int32_t n_parts, int32_t* part,
+              int64_t* part_cost) {
     std::vector<int64_t> cost(n_windows);
     for (int32_t w = 0; w < n_windows; w++) {
         if (win_off[w + 1] < win_off[w]) return POA_BAD_ARG;
@@ -54,6 +68,8 @@ extern "C" int poa_batch_partition(const int32_t* read_len, const int32_t* win_o
         for (int32_t g = 0; g < n_parts; g++) part_cost[g] = load[g];
     return POA_OK;
 }
+
+}  // namespace
 
 namespace {
 

@@ -228,3 +228,23 @@ def test_batch_rows_with_many_predecessors(opts, oracle_bin, tmp_path):
         synth.write_fasta(str(fa), rs)
         want = _cons_of(subprocess.run([oracle_bin, str(fa)] + opts, capture_output=True, check=True).stdout)
         assert st[w] == 0 and cons[w] == want
+
+
+@pytest.mark.parametrize("opts,smem", [([], 0), (["-B"], 0), (["-B"], 10240)],
+                         ids=["static", "adaptive", "adaptive_query_in_slot"])
+def test_batch_long_reads(opts, smem, oracle_bin, tmp_path):
+    """Windows of 9-12 kb reads at 10 % error. With 10 KB of shared memory per
+    warp the adaptive fill cannot stage a 12 kb query next to its records and
+    reads it from the slot instead; every variant must print the reference's
+    consensus."""
+    ws = synth.windows(51, 2, (9000, 12000), (5, 6), 0.10)
+    with poa_b200.Context(poa_b200.Params.from_cli(opts)) as ctx:
+        if smem:
+            ctx.batch_config(smem_per_warp=smem)
+        cons, st = ctx.batch_consensus(ws)
+    for w in range(ws.n_windows):
+        fa = tmp_path / f"w{w}.fa"
+        synth.write_fasta(str(fa), ws.window_reads(w))
+        want = subprocess.run([oracle_bin, str(fa)] + opts, capture_output=True, check=True, timeout=900).stdout
+        assert st[w] == 0
+        assert cons[w] == _cons_of(want), w

@@ -121,6 +121,9 @@ class Dist:
             import torch
             import torch.distributed as dist
             backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if torch.cuda.is_available():
+                # this rank's GPU before the group exists, so every collective runs on it
+                torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.pg = dist
 
